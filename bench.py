@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Fluid MLUPS of the fused D3Q27 stream + collide step on one B200 (and N replicas).
+
+Workload (one time step = one "step"): the synthetic TCPC junction 256x192x160, FP32
+storage, cumulant collision, Carreau-Yasuda viscosity from the non-equilibrium moments,
+plug IVC/SVC inflow, rho = 1 outlets, FP64 mean/rms accumulators on.  The junction is
+sparse (about 5 % fluid), so the data one step touches fits in the 126 MB L2: every timed
+step is preceded by a 512 MB buffer write that flushes L2, and steps are timed one by one
+with CUDA events on the library's stream.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                    [--dtype f32|f16|bf16|f64] [--collision CUM] [--no-stats]
+
+Multi-GPU (launched by torchrun, one rank per GPU): every rank runs its own replica of the
+case (the path has no exchange step on one GPU); value = all fluid-cell updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "fluid MLUPS & %HBM roofline; FP16 vs FP32 storage at stated error; batch gain"
+STORAGE_BYTES = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--dtype", default="f32")
+    ap.add_argument("--collision", default="CUM")
+    ap.add_argument("--cy-mode", default="local-neq")
+    ap.add_argument("--no-stats", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=400)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self):
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower().startswith("active"):
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(key: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get(key)
+    return None
+
+
+def bytes_per_update(dtype: str, stats: bool, stats_f64: bool = True) -> float:
+    """Algorithmic bytes per fluid-cell update: 27 reads + 27 writes of the populations,
+    the 1-byte label, and the mean/rms sums (6 read + 6 written)."""
+    b = 2 * 27 * STORAGE_BYTES[dtype] + 1
+    if stats:
+        b += 2 * 6 * (8 if stats_f64 else 4)
+    return float(b)
+
+
+def run_reference(a, dist: Dist):
+    """The reference's own collision/streaming headers (oracle/_ref, single precision like
+    the production build) driven by the single-rank host loop, on the same lattice."""
+    if dist.rank != 0:
+        return 0
+    import oracle as O
+    from nonnewlbm_b200 import geometry as G
+    from nonnewlbm_b200 import workloads as W
+
+    if not O.ref_available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnnlbm_ref_fast.so not built "
+                          "(the reference checkout was absent at build time)"}))
+        return 0
+    w = W.junction_cy(dtype="f32", collision=a.collision)
+    nx, ny, nz = w.shape
+    lib = O.ref_lib(fast=True)
+    threads = os.cpu_count() or 1
+    lib.ref_set_threads(threads)
+    orc = O.Oracle(nx, ny, nz)
+    rc, counts = orc.setup_tcpc(w.wall)
+    m = orc.get_map()
+    del orc
+    ref = O.RefLattice(nx, ny, nz, collision=O.COLLISIONS.index(a.collision), equilibrium=O.EQ_INV_CUM_REF, nu=w.nu,
+                       prec=4, fast=True)
+    ref.set_map(m)
+    ref.set_inflow(ivc_flux=w.u_ivc * counts[0], svc_flux=w.u_svc * counts[1])
+    ref.init_equilibrium()
+    fluid = int(np.count_nonzero((m == G.MAP_FLUID) | (m == G.MAP_PERIODIC)))
+    for _ in range(max(1, min(a.warmup, 2))):
+        ref.step(1, accumulate_stats=not a.no_stats)
+    times = []
+    t_end = time.perf_counter() + a.cpu_seconds
+    steps = 0
+    while steps < max(1, a.steps) and (time.perf_counter() < t_end or steps < 2):
+        t0 = time.perf_counter()
+        ref.step(1, accumulate_stats=not a.no_stats)
+        times.append(time.perf_counter() - t0)
+        steps += 1
+    sec = float(np.mean(times))
+    mlups = fluid / sec / 1e6
+    sample = (f"{steps} steps of the full {nx}x{ny}x{nz} junction (fluid {fluid} cells) on {threads} host threads, "
+              f"reference cumulant + streaming headers in single precision (TraitsSP); the single-rank reference "
+              f"leaves Carreau-Yasuda inert (zero strain), so the Newtonian step is timed")
+    line = {"impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": a.gpus,
+            "steps": steps, "warmup": max(1, min(a.warmup, 2)), "ms_per_step": round(sec * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "timing": "per-step CUDA events, L2 flushed (512 MB write) before every step", "collision": a.collision, "storage": "f32 (reference TraitsSP)",
+                       "cells": nx * ny * nz, "fluid_cells": fluid},
+            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline_sample(w, seconds: float, collision: str) -> dict:
+    import oracle as O
+    from nonnewlbm_b200 import geometry as G
+
+    if not O.ref_available(fast=True):
+        return {"value": None, "unit": "MLUPS", "cores": 0, "kind": "reference", "sample": "oracle/_ref not built"}
+    nx, ny, nz = w.shape
+    lib = O.ref_lib(fast=True)
+    threads = os.cpu_count() or 1
+    lib.ref_set_threads(threads)
+    orc = O.Oracle(nx, ny, nz)
+    rc, counts = orc.setup_tcpc(w.wall)
+    m = orc.get_map()
+    del orc
+    ref = O.RefLattice(nx, ny, nz, collision=O.COLLISIONS.index(collision), nu=w.nu, prec=4, fast=True)
+    ref.set_map(m)
+    ref.set_inflow(ivc_flux=w.u_ivc * counts[0], svc_flux=w.u_svc * counts[1])
+    ref.init_equilibrium()
+    ref.step(1)
+    fluid = int(np.count_nonzero((m == G.MAP_FLUID) | (m == G.MAP_PERIODIC)))
+    t0 = time.perf_counter()
+    n = 0
+    while n < 2 or time.perf_counter() - t0 < seconds:
+        ref.step(1)
+        n += 1
+    sec = (time.perf_counter() - t0) / n
+    return {"value": round(fluid / sec / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": "reference",
+            "sample": f"{n} steps of the same junction ({fluid} fluid cells), reference headers in single precision, "
+                      f"{threads} OpenMP threads; Carreau-Yasuda inert as in the single-rank reference"}
+
+
+def main() -> int:
+    a = parse()
+    dist = Dist()
+    dist.init()
+    try:
+        if a.impl == "reference":
+            return run_reference(a, dist)
+        return run_ours(a, dist)
+    finally:
+        dist.close()
+
+
+def run_ours(a, dist: Dist) -> int:
+    import torch
+
+    from nonnewlbm_b200 import capi
+    from nonnewlbm_b200 import workloads as W
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    stats = not a.no_stats
+    w = W.junction_cy(dtype=a.dtype, collision=a.collision, cy_mode=a.cy_mode)
+    lat = W.build_lattice(w, device=dev)
+    info = lat.step_info()
+    lat.autotune()
+    stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+    lat.step(max(3, a.warmup), stats=stats)
+    # the populations touched per step can be smaller than the 126 MB L2 (a sparse
+    # junction): every timed step starts from a cold L2 by writing a 512 MB buffer first,
+    # outside the step's events
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{dev}")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    sampler = ClockSampler(dev)
+    sampler.start()
+    time.sleep(0.3)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream):
+        for k in range(a.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            lat.step(1, stats=stats)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    clocks = sampler.stop()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
+    ms = dist.max(ms)
+    fluid = info["fluid_cells"]
+    value = fluid * a.steps * dist.world / (ms / 1e3) / 1e6
+
+    # dominant kernel: per-launch device time with events around every kernel
+    prof = lat.profile_step(20, stats=stats)
+    t_step_ms = prof["step"][0]
+    bpu = bytes_per_update(a.dtype, stats)
+    peak, peak_kind = measured_peaks()
+    achieved = fluid * bpu / (t_step_ms / 1e3) / 1e9
+    key = f"{w.name}:{a.dtype}:{a.collision}:{a.cy_mode}:{'stats' if stats else 'nostats'}"
+    traffic = ncu_traffic(key)
+
+    # end to end through the public API: per step the host sends that step's inflow row
+    # (pinned staging inside the library) and reads back the FP64 mass / flux sums
+    rows = np.array([[w.u_ivc * w.notes["counts"]["left_area"], w.u_svc * w.notes["counts"]["right_area"], 1.0]])
+    dist.barrier()
+    t0 = time.perf_counter()
+    red = None
+    for _ in range(a.e2e_steps):
+        lat.set_schedule(rows)
+        lat.step(1, stats=stats, reduce=True)
+        red = lat.reduce()
+    t_e2e = time.perf_counter() - t0
+    t_e2e = dist.max(t_e2e)
+    e2e = fluid * a.e2e_steps * dist.world / t_e2e / 1e6
+    ctl_bytes = 32 if w.dtype != "f64" else 56
+    h2d = ctl_bytes + 8  # the step's control row + the cursor reset
+    d2h = 5 * 8 + 3 * 4  # mass/flux sums + the watchdog / cursor words
+
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": dist.world, "steps": a.steps,
+            "warmup": max(3, a.warmup), "ms_per_step": round(ms / a.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": a.dtype, "data": "synthetic",
+            "config": {"workload": w.name, "timing": "per-step CUDA events, L2 flushed (512 MB write) before every step", "shape": list(w.shape), "fluid_cells": fluid, "collision": a.collision,
+                       "cy_mode": a.cy_mode, "storage": a.dtype, "stats": "fp64 mean/rms" if stats else "off",
+                       "bc_cells": info["bc_cells"], "parallelism": f"replicas x{dist.world}",
+                       "dt_s": w.notes.get("dt_s"), "dx_m": w.notes.get("dx_m")},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": f"k_step<{a.dtype},{a.collision}>", "bytes_per_update": bpu,
+                         "kernel_ms": round(t_step_ms, 5),
+                         "step_kernels_ms": {k: round(v[0], 5) for k, v in prof.items() if v[1]}},
+            "e2e": {"value": round(e2e, 2), "unit": "MLUPS", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": a.steps * info["launches_per_step"],
+            "clocks": clocks,
+        }
+        if dist.world == 1:
+            line["cpu_baseline"] = cpu_baseline_sample(w, a.cpu_seconds, a.collision)
+        line["reduce_last"] = [float(v) for v in red] if red is not None else None
+        print(json.dumps(line))
+    lat.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

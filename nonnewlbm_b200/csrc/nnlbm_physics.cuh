@@ -1,0 +1,465 @@
+// nnlbm_physics.cuh -- per-cell D3Q27 physics for the sm_100a step kernels.
+//
+// Direction q = 9*(cx+1) + 3*(cy+1) + (cz+1) (the reference enum, solver/lbm3d/defs.h:215-247),
+// opposite direction 26-q.  CT is the arithmetic type: float for F32/F16/BF16 storage and
+// double for F64 storage.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace nnlbm {
+
+__host__ __device__ constexpr int cxq(int q) { return q / 9 - 1; }
+__host__ __device__ constexpr int cyq(int q) { return (q / 3) % 3 - 1; }
+__host__ __device__ constexpr int czq(int q) { return q % 3 - 1; }
+__host__ __device__ constexpr int oppq(int q) { return 26 - q; }
+__host__ __device__ constexpr int nnzq(int q) { return (cxq(q) != 0) + (cyq(q) != 0) + (czq(q) != 0); }
+
+// lattice weights 8/27, 2/27, 1/54, 1/216 by the number of non-zero velocity components
+template <class CT>
+__host__ __device__ constexpr CT weight(int q)
+{
+    return nnzq(q) == 0 ? CT(8.0 / 27.0) : nnzq(q) == 1 ? CT(2.0 / 27.0) : nnzq(q) == 2 ? CT(1.0 / 54.0) : CT(1.0 / 216.0);
+}
+
+enum : int { EQ_INV_CUM_REF = 0, EQ_INV_CUM = 1, EQ_DEFAULT = 2, EQ_ENTROPIC = 3 };
+enum : int { COL_CUM = 0, COL_KBC_N1 = 1, COL_KBC_N2, COL_KBC_N3, COL_KBC_N4, COL_KBC_C1, COL_KBC_C2,
+             COL_KBC_C3, COL_KBC_C4, COL_MRT = 9, COL_BGK = 10 };
+
+template <class CT> __device__ __forceinline__ CT dsqrt(CT v);
+template <> __device__ __forceinline__ float dsqrt<float>(float v) { return sqrtf(v); }
+template <> __device__ __forceinline__ double dsqrt<double>(double v) { return sqrt(v); }
+template <class CT> __device__ __forceinline__ CT dpow(CT b, CT e);
+template <> __device__ __forceinline__ float dpow<float>(float b, float e) { return powf(b, e); }
+template <> __device__ __forceinline__ double dpow<double>(double b, double e) { return pow(b, e); }
+
+// ---------------------------------------------------------------------------------------
+// density and velocity with the F/2 shift, in the pairwise order of Geier 2015 Appendix J
+// (the order of LBM_COMMON::computeDensityAndVelocity, solver/lbm3d/lbm_common.h:31-38)
+// ---------------------------------------------------------------------------------------
+template <class CT>
+__device__ __forceinline__ void density_velocity(const CT* f, CT fx, CT fy, CT fz, CT& rho, CT& ux, CT& uy, CT& uz)
+{
+    enum { mmm = 0, mmz, mmp, mzm, mzz, mzp, mpm, mpz, mpp, zmm, zmz, zmp, zzm, zzz, zzp, zpm, zpz, zpp,
+           pmm, pmz, pmp, pzm, pzz, pzp, ppm, ppz, ppp };
+    rho = ((((f[ppp] + f[mmm]) + (f[pmp] + f[mpm])) + ((f[ppm] + f[mmp]) + (f[mpp] + f[pmm])))
+           + (((f[zpp] + f[zmm]) + (f[zpm] + f[zmp])) + ((f[pzp] + f[mzm]) + (f[pzm] + f[mzp]))
+              + ((f[ppz] + f[mmz]) + (f[pmz] + f[mpz])))
+           + ((f[pzz] + f[mzz]) + (f[zpz] + f[zmz]) + (f[zzp] + f[zzm]))) + f[zzz];
+    const CT ir = CT(1) / rho;
+    uz = ((((f[ppp] - f[mmm]) + (f[mpp] - f[pmm])) + ((f[pmp] - f[mpm]) + (f[mmp] - f[ppm])))
+          + (((f[zpp] - f[zmm]) + (f[zmp] - f[zpm])) + ((f[pzp] - f[mzm]) + (f[mzp] - f[pzm])))
+          + (f[zzp] - f[zzm]) + fz * CT(0.5)) * ir;
+    ux = ((((f[ppp] - f[mmm]) + (f[pmp] - f[mpm])) + ((f[ppm] - f[mmp]) + (f[pmm] - f[mpp])))
+          + (((f[pzp] - f[mzm]) + (f[pzm] - f[mzp])) + ((f[ppz] - f[mmz]) + (f[pmz] - f[mpz])))
+          + (f[pzz] - f[mzz]) + fx * CT(0.5)) * ir;
+    uy = ((((f[ppp] - f[mmm]) + (f[ppm] - f[mmp])) + ((f[mpp] - f[pmm]) + (f[mpm] - f[pmp])))
+          + (((f[ppz] - f[mmz]) + (f[mpz] - f[pmz])) + ((f[zpp] - f[zmm]) + (f[zpm] - f[zmp])))
+          + (f[zpz] - f[zmz]) + fy * CT(0.5)) * ir;
+}
+
+template <class CT>
+__device__ __forceinline__ CT density(const CT* f)
+{
+    CT r, a, b, c;
+    density_velocity<CT>(f, CT(0), CT(0), CT(0), r, a, b, c);
+    return r;
+}
+
+// ---------------------------------------------------------------------------------------
+// equilibria for boundary nodes and initial states
+// ---------------------------------------------------------------------------------------
+template <class CT>
+__device__ __forceinline__ CT inv_cum_factor(int c, CT v)
+{
+    return c == 0 ? CT(3) * v * v - CT(2) : (c > 0 ? CT(3) * v * v + CT(3) * v + CT(1) : CT(3) * v * v - CT(3) * v + CT(1));
+}
+
+// feq of kind `eq` (runtime-uniform switch) into f[27]
+template <class CT>
+__device__ void equilibrium(int eq, CT rho, CT ux, CT uy, CT uz, CT* f)
+{
+    if (eq == EQ_DEFAULT) {
+        // LBM_EQ_DEFAULT, lbm_eq.h:12-47
+        const CT u2 = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const CT cu = CT(cxq(q)) * ux + CT(cyq(q)) * uy + CT(czq(q)) * uz;
+            f[q] = weight<CT>(q) * rho * (CT(1) - CT(1.5) * u2 + CT(3) * cu + CT(4.5) * cu * cu);
+        }
+    } else if (eq == EQ_ENTROPIC) {
+        // LBM_EQ_ENTROPIC, lbm_eq_entropic.h:12-38: per axis weight (2/3 or 1/6) times
+        // (2 - sqrt(1+3v^2)) times B^c with B = (2v + sqrt(1+3v^2)) / (1 - v)
+        const CT sx = dsqrt<CT>(CT(1) + CT(3) * ux * ux), sy = dsqrt<CT>(CT(1) + CT(3) * uy * uy);
+        const CT sz = dsqrt<CT>(CT(1) + CT(3) * uz * uz);
+        const CT bx = (CT(2) * ux + sx) / (CT(1) - ux), by = (CT(2) * uy + sy) / (CT(1) - uy), bz = (CT(2) * uz + sz) / (CT(1) - uz);
+        const CT base = (CT(2) - sx) * (CT(2) - sy) * (CT(2) - sz);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            CT v = (cxq(q) ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) * (cyq(q) ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) *
+                   (czq(q) ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) * base;
+            if (cxq(q) > 0) v *= bx; else if (cxq(q) < 0) v *= CT(1) / bx;
+            if (cyq(q) > 0) v *= by; else if (cyq(q) < 0) v *= CT(1) / by;
+            if (czq(q) > 0) v *= bz; else if (czq(q) < 0) v *= CT(1) / bz;
+            f[q] = rho * v;
+        }
+    } else {
+        // factorised equilibrium of LBM_EQ_INV_CUM (lbm_eq_inv_cum.h:71-101): prefactor by
+        // the number of zero components 3: -1/27, 2: 1/54, 1: -1/108, 0: 1/216
+        CT X[3], Y[3], Z[3];
+#pragma unroll
+        for (int c = -1; c <= 1; ++c) {
+            X[c + 1] = inv_cum_factor<CT>(c, ux);
+            Y[c + 1] = inv_cum_factor<CT>(c, uy);
+            Z[c + 1] = inv_cum_factor<CT>(c, uz);
+        }
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const int nz0 = nnzq(q);
+            const CT pre = nz0 == 0 ? CT(-1.0 / 27.0) : nz0 == 1 ? CT(1.0 / 54.0) : nz0 == 2 ? CT(-1.0 / 108.0) : CT(1.0 / 216.0);
+            f[q] = pre * rho * (X[cxq(q) + 1] * Y[cyq(q) + 1] * Z[czq(q) + 1]);
+        }
+        // the shipped feq_pmm multiplies by rho twice (lbm_eq_inv_cum.h:49)
+        if (eq == EQ_INV_CUM_REF) f[18] *= rho;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// cumulant collision (Geier et al. 2015) with the reference configuration of
+// solver/lbm3d/lbm_col_cum.h:166-282: shear rate omega1 = 1/(3 nu + 1/2), every other rate
+// 1, A = B = 0, no limiter.  With those rates all cumulants of order >= 3 are reset to
+// zero, so only the central moments up to second order are needed from the forward
+// transform; the backward transform rebuilds orders 4..6 from products of second order
+// ones (G2015 Eq 81-84).
+// ---------------------------------------------------------------------------------------
+template <class CT>
+__device__ __forceinline__ void fwd3(CT m, CT z, CT p, CT u, CT& k0, CT& k1, CT& k2)
+{
+    k0 = (p + m) + z;
+    k1 = (p - m) - u * k0;
+    k2 = (p + m) - CT(2) * u * (p - m) + u * u * k0;
+}
+
+template <class CT>
+__device__ __forceinline__ void bwd3(CT k0, CT k1, CT k2, CT u, CT& m, CT& z, CT& p)
+{
+    z = k0 * (CT(1) - u * u) - CT(2) * u * k1 - k2;
+    m = (k0 * (u * u - u) + k1 * (CT(2) * u - CT(1)) + k2) * CT(0.5);
+    p = (k0 * (u * u + u) + k1 * (CT(2) * u + CT(1)) + k2) * CT(0.5);
+}
+
+template <class CT>
+__device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu)
+{
+    // forward: z pass over the 9 (x,y) columns
+    CT a[3][3][3];
+#pragma unroll
+    for (int ix = 0; ix < 3; ++ix)
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy)
+            fwd3<CT>(f[9 * ix + 3 * iy], f[9 * ix + 3 * iy + 1], f[9 * ix + 3 * iy + 2], uz, a[ix][iy][0], a[ix][iy][1], a[ix][iy][2]);
+    // y pass
+    CT b[3][3][3];
+#pragma unroll
+    for (int ix = 0; ix < 3; ++ix)
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz)
+            fwd3<CT>(a[ix][0][kz], a[ix][1][kz], a[ix][2][kz], uy, b[ix][0][kz], b[ix][1][kz], b[ix][2][kz]);
+    // x pass, only the moments of total order <= 2 are used below
+    CT k[3][3][3];
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz)
+            if (ky + kz <= 2) fwd3<CT>(b[0][ky][kz], b[1][ky][kz], b[2][ky][kz], ux, k[0][ky][kz], k[1][ky][kz], k[2][ky][kz]);
+
+    const CT ir = CT(1) / rho;
+    const CT om = CT(1) / (CT(3) * nu + CT(0.5));
+    const CT k000 = k[0][0][0];
+    // relaxation (lbm_col_cum.h:205-235 with omega2 = 1 and no anti-aliasing terms)
+    const CT s110 = (CT(1) - om) * k[1][1][0];
+    const CT s101 = (CT(1) - om) * k[1][0][1];
+    const CT s011 = (CT(1) - om) * k[0][1][1];
+    const CT e33 = (CT(1) - om) * (k[2][0][0] - k[0][2][0]);
+    const CT e34 = (CT(1) - om) * (k[2][0][0] - k[0][0][2]);
+    const CT s200 = CT(1.0 / 3.0) * (e33 + e34 + k000);
+    const CT s020 = CT(1.0 / 3.0) * (CT(-2) * e33 + e34 + k000);
+    const CT s002 = CT(1.0 / 3.0) * (e33 - CT(2) * e34 + k000);
+    // fourth order from products (Eq 81-82); third and fifth order vanish
+    const CT s211 = (s200 * s011 + CT(2) * s101 * s110) * ir;
+    const CT s121 = (s020 * s101 + CT(2) * s110 * s011) * ir;
+    const CT s112 = (s002 * s110 + CT(2) * s011 * s101) * ir;
+    const CT s220 = (s020 * s200 + CT(2) * s110 * s110) * ir;
+    const CT s022 = (s002 * s020 + CT(2) * s011 * s011) * ir;
+    const CT s202 = (s200 * s002 + CT(2) * s101 * s101) * ir;
+    // sixth order (Eq 84 with the odd orders at zero)
+    const CT s222 = (s200 * s022 + s020 * s202 + s002 * s220 + CT(4) * (s011 * s211 + s101 * s121 + s110 * s112)) * ir
+                    - (CT(16) * s110 * s101 * s011 + CT(4) * (s101 * s101 * s020 + s011 * s011 * s200 + s110 * s110 * s002)
+                       + CT(2) * s200 * s020 * s002) * ir * ir;
+
+    CT s[3][3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int l = 0; l < 3; ++l) s[i][j][l] = CT(0);
+    s[0][0][0] = k000;
+    s[1][0][0] = -k[1][0][0]; s[0][1][0] = -k[0][1][0]; s[0][0][1] = -k[0][0][1];
+    s[1][1][0] = s110; s[1][0][1] = s101; s[0][1][1] = s011;
+    s[2][0][0] = s200; s[0][2][0] = s020; s[0][0][2] = s002;
+    s[2][1][1] = s211; s[1][2][1] = s121; s[1][1][2] = s112;
+    s[2][2][0] = s220; s[0][2][2] = s022; s[2][0][2] = s202;
+    s[2][2][2] = s222;
+    // backward: x, y, z (G2015 Eq 88-96)
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz)
+            bwd3<CT>(s[0][ky][kz], s[1][ky][kz], s[2][ky][kz], ux, b[0][ky][kz], b[1][ky][kz], b[2][ky][kz]);
+#pragma unroll
+    for (int ix = 0; ix < 3; ++ix)
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz)
+            bwd3<CT>(b[ix][0][kz], b[ix][1][kz], b[ix][2][kz], uy, a[ix][0][kz], a[ix][1][kz], a[ix][2][kz]);
+#pragma unroll
+    for (int ix = 0; ix < 3; ++ix)
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy)
+            bwd3<CT>(a[ix][iy][0], a[ix][iy][1], a[ix][iy][2], uz, f[9 * ix + 3 * iy], f[9 * ix + 3 * iy + 1], f[9 * ix + 3 * iy + 2]);
+}
+
+// ---------------------------------------------------------------------------------------
+// factorised equilibrium of the BGK / KBC schemes (lbm_col_bgk.h:43-53, 85-111):
+// feq_q = -rho X_cx Y_cy Z_cz with Xz = u^2 - 2/3, Xp = -(u^2 + u + 1/3)/2, Xm = Xp + u
+// ---------------------------------------------------------------------------------------
+template <class CT>
+struct FactEq {
+    CT X[3], Y[3], Z[3];
+    __device__ __forceinline__ FactEq(CT ux, CT uy, CT uz)
+    {
+        X[1] = CT(1.0 / 3.0) - CT(1) + ux * ux; X[2] = CT(-0.5) * (X[1] + CT(1) + ux); X[0] = X[2] + ux;
+        Y[1] = CT(1.0 / 3.0) - CT(1) + uy * uy; Y[2] = CT(-0.5) * (Y[1] + CT(1) + uy); Y[0] = Y[2] + uy;
+        Z[1] = CT(1.0 / 3.0) - CT(1) + uz * uz; Z[2] = CT(-0.5) * (Z[1] + CT(1) + uz); Z[0] = Z[2] + uz;
+    }
+    __device__ __forceinline__ CT operator()(int q, CT rho) const { return -rho * X[q / 9] * Y[(q / 3) % 3] * Z[q % 3]; }
+};
+
+// forcing source S_q of lbm_col_bgk.h:57-83
+template <class CT>
+__device__ __forceinline__ CT force_src(int q, CT ir, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz)
+{
+    return (CT(3) * ((CT(cxq(q)) - ux) * fx + (CT(cyq(q)) - uy) * fy + (CT(czq(q)) - uz) * fz)) * ir;
+}
+
+// BGK, solver/lbm3d/lbm_col_bgk.h:14-140
+template <class CT>
+__device__ __forceinline__ void collide_bgk(CT* f, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz, CT nu)
+{
+    const CT om = CT(1) / (CT(3) * nu + CT(0.5));
+    const CT ir = CT(1) / rho;
+    const FactEq<CT> E(ux, uy, uz);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const CT feq = E(q, rho);
+        f[q] += (feq - f[q]) * om + (CT(1) - CT(0.5) * om) * force_src<CT>(q, ir, ux, uy, uz, fx, fy, fz) * feq;
+    }
+}
+
+// MRT_LES, solver/lbm3d/lbm_col_mrt.h:12-78: second moments relaxed with a Smagorinsky rate,
+// everything rebuilt as w_q [rho (1 + 3 c.u) + 9/2 (c c - I/3) : (P - rho I/3)] form
+template <class CT>
+__device__ __forceinline__ void collide_mrt(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu)
+{
+    CT Pxx = 0, Pyy = 0, Pzz = 0, Pxy = 0, Pxz = 0, Pyz = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const int cx = cxq(q), cy = cyq(q), cz = czq(q);
+        if (cx) Pxx += f[q];
+        if (cy) Pyy += f[q];
+        if (cz) Pzz += f[q];
+        if (cx * cy > 0) Pxy += f[q]; else if (cx * cy < 0) Pxy -= f[q];
+        if (cx * cz > 0) Pxz += f[q]; else if (cx * cz < 0) Pxz -= f[q];
+        if (cy * cz > 0) Pyz += f[q]; else if (cy * cz < 0) Pyz -= f[q];
+    }
+    const CT Pnxx = Pxx - rho * (CT(1.0 / 3.0) + ux * ux);
+    const CT Pnyy = Pyy - rho * (CT(1.0 / 3.0) + uy * uy);
+    const CT Pnzz = Pzz - rho * (CT(1.0 / 3.0) + uz * uz);
+    const CT Pnxz = Pxz - rho * ux * uz;
+    const CT Pnxy = Pxy - rho * ux * uy;
+    const CT Pnyz = Pyz - rho * uy * uz;
+    const CT Qs = CT(2) * (Pnxx * Pnxx + Pnyy * Pnyy + Pnzz * Pnzz + CT(2) * (Pnxy * Pnxy + Pnxz * Pnxz + Pnyz * Pnyz));
+    const CT tau = CT(3) * nu + CT(0.5);
+    const CT om = CT(2) / (dsqrt<CT>(tau * tau + CT(2) * CT(0.0342) * CT(9) * dsqrt<CT>(Qs) / rho) + tau);
+    Pxx -= om * Pnxx; Pyy -= om * Pnyy; Pzz -= om * Pnzz;
+    Pxy -= om * Pnxy; Pxz -= om * Pnxz; Pyz -= om * Pnyz;
+    const CT tr = Pxx + Pyy + Pzz;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const int cx = cxq(q), cy = cyq(q), cz = czq(q);
+        const int c2 = cx * cx + cy * cy + cz * cz;
+        const CT cu = CT(cx) * ux + CT(cy) * uy + CT(cz) * uz;
+        const CT pp = CT(cx * cx) * Pxx + CT(cy * cy) * Pyy + CT(cz * cz) * Pzz
+                      + CT(2) * (CT(cx * cy) * Pxy + CT(cx * cz) * Pxz + CT(cy * cz) * Pyz);
+        f[q] = weight<CT>(q) * (rho * (CT(2.5) - CT(1.5) * CT(c2) + CT(3) * cu) + CT(4.5) * pp - CT(1.5) * tr);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// KBC (Karlin, Boesch, Chikatamarla 2015), lbm_col_kbc_n.h / lbm_col_kbc_c.h: shear part
+// s = D [+T] [+Q] of raw (N) or central (C) moments, entropic stabiliser gamma,
+// f -= beta (2 ds + gamma dh) - (1-beta) S feq.  Two passes over q keep the per-direction
+// temporaries out of registers.
+// ---------------------------------------------------------------------------------------
+template <class CT>
+struct KbcMom { CT T, Nxz, Nyz, Pxy, Pxz, Pyz, Qxxy, Qxxz, Qxyy, Qyyz, Qxzz, Qyzz, Qxyz; };
+
+template <class CT, bool USE_T, bool USE_Q>
+__device__ __forceinline__ CT kbc_shear(int q, const KbcMom<CT>& m)
+{
+    const int cx = cxq(q), cy = cyq(q), cz = czq(q), nz0 = nnzq(q);
+    CT D = 0, T = 0, Qv = 0;
+    if (nz0 == 1) {
+        if (cx) D = (CT(2) * m.Nxz - m.Nyz) * CT(1.0 / 6.0);
+        if (cy) D = (-m.Nxz + CT(2) * m.Nyz) * CT(1.0 / 6.0);
+        if (cz) D = (-m.Nxz - m.Nyz) * CT(1.0 / 6.0);
+        T = m.T * CT(1.0 / 6.0);
+        if (cx) Qv = CT(-cx) * (m.Qxyy + m.Qxzz) * CT(0.5);
+        if (cy) Qv = CT(-cy) * (m.Qxxy + m.Qyzz) * CT(0.5);
+        if (cz) Qv = CT(-cz) * (m.Qxxz + m.Qyyz) * CT(0.5);
+    } else if (nz0 == 2) {
+        if (!cz) { D = CT(cx * cy) * m.Pxy * CT(0.25); Qv = (CT(cx) * m.Qxyy + CT(cy) * m.Qxxy) * CT(0.25); }
+        if (!cy) { D = CT(cx * cz) * m.Pxz * CT(0.25); Qv = (CT(cx) * m.Qxzz + CT(cz) * m.Qxxz) * CT(0.25); }
+        if (!cx) { D = CT(cy * cz) * m.Pyz * CT(0.25); Qv = (CT(cy) * m.Qyzz + CT(cz) * m.Qyyz) * CT(0.25); }
+    } else if (nz0 == 3) {
+        Qv = CT(cx * cy * cz) * m.Qxyz * CT(0.125);
+    } else {
+        T = -m.T;
+    }
+    return D + (USE_T ? T : CT(0)) + (USE_Q ? Qv : CT(0));
+}
+
+template <class CT, bool CENTRAL, bool USE_T, bool USE_Q>
+__device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz, CT nu)
+{
+    CT M200 = 0, M020 = 0, M002 = 0, M110 = 0, M101 = 0, M011 = 0, M111 = 0;
+    CT M201 = 0, M102 = 0, M210 = 0, M120 = 0, M021 = 0, M012 = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const int cx = cxq(q), cy = cyq(q), cz = czq(q);
+        const CT v = f[q];
+        if (cx) { M200 += v; if (cz) M201 += CT(cz) * v; if (cy) M210 += CT(cy) * v; }
+        if (cy) { M020 += v; if (cz) M021 += CT(cz) * v; if (cx) M120 += CT(cx) * v; }
+        if (cz) { M002 += v; if (cx) M102 += CT(cx) * v; if (cy) M012 += CT(cy) * v; }
+        if (cx && cy) M110 += CT(cx * cy) * v;
+        if (cx && cz) M101 += CT(cx * cz) * v;
+        if (cy && cz) M011 += CT(cy * cz) * v;
+        if (cx && cy && cz) M111 += CT(cx * cy * cz) * v;
+    }
+    const CT cs2 = CT(1.0 / 3.0);
+    KbcMom<CT> m, e;
+    const CT rT = M200 + M020 + M002, rNxz = M200 - M002, rNyz = M020 - M002;
+    if (!CENTRAL) {
+        m = {rT, rNxz, rNyz, M110, M101, M011, M210, M201, M120, M021, M102, M012, M111};
+        e.T = rho * (CT(3) * cs2 + ux * ux + uy * uy + uz * uz);
+        e.Nxz = rho * (ux * ux - uz * uz); e.Nyz = rho * (uy * uy - uz * uz);
+        e.Pxy = rho * ux * uy; e.Pxz = rho * ux * uz; e.Pyz = rho * uy * uz;
+        e.Qxxy = rho * uy * (cs2 + ux * ux); e.Qxxz = rho * uz * (cs2 + ux * ux);
+        e.Qxyy = rho * ux * (cs2 + uy * uy); e.Qyyz = rho * uz * (cs2 + uy * uy);
+        e.Qxzz = rho * ux * (cs2 + uz * uz); e.Qyzz = rho * uy * (cs2 + uz * uz);
+        e.Qxyz = rho * ux * uy * uz;
+    } else {
+        const CT cT = rT - rho * (ux * ux + uy * uy + uz * uz);
+        const CT cNxz = rNxz + rho * (uz * uz - ux * ux), cNyz = rNyz + rho * (uz * uz - uy * uy);
+        const CT cPxy = M110 - rho * ux * uy, cPxz = M101 - rho * ux * uz, cPyz = M011 - rho * uy * uz;
+        m.T = cT; m.Nxz = cNxz; m.Nyz = cNyz; m.Pxy = cPxy; m.Pxz = cPxz; m.Pyz = cPyz;
+        m.Qxxy = M210 - CT(1.0 / 3.0) * (CT(6) * ux * cPxy + uy * (CT(3) * ux * ux + CT(2) * cNxz - cNyz + cT));
+        m.Qxxz = M201 - CT(1.0 / 3.0) * (CT(6) * ux * cPxz + uz * (CT(3) * ux * ux + CT(2) * cNxz - cNyz + cT));
+        m.Qxyy = M120 - CT(1.0 / 3.0) * (CT(6) * uy * cPxy + ux * (CT(3) * uy * uy + CT(2) * cNyz - cNxz + cT));
+        m.Qyyz = M021 - CT(1.0 / 3.0) * (CT(6) * uy * cPyz + uz * (CT(3) * uy * uy + CT(2) * cNyz - cNxz + cT));
+        m.Qxzz = M102 - CT(1.0 / 3.0) * (CT(6) * uz * cPxz + ux * (CT(3) * uz * uz - cNyz - cNxz + cT));
+        m.Qyzz = M012 - CT(1.0 / 3.0) * (CT(6) * uz * cPyz + uy * (CT(3) * uz * uz - cNyz - cNxz + cT));
+        m.Qxyz = M111 - ux * cPyz - uy * cPxz - uz * cPxy - ux * uy * uz;
+        e = {rho * CT(3) * cs2, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    }
+    const FactEq<CT> E(ux, uy, uz);
+    const CT beta = CT(1) / (CT(2) * nu / cs2 + CT(1));
+    CT num = 0, den = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const CT feq = E(q, rho);
+        const CT ds = kbc_shear<CT, USE_T, USE_Q>(q, m) - kbc_shear<CT, USE_T, USE_Q>(q, e);
+        const CT dh = f[q] - feq - ds;
+        const CT ifeq = CT(1) / feq;
+        num += ds * dh * ifeq;
+        den += dh * dh * ifeq;
+    }
+    // the reference divides 0/0 when dh vanishes identically; gamma*dh is then zero for any
+    // finite gamma and the regularised limit 1/beta is taken
+    const CT gamma = den != CT(0) ? CT(1) / beta - (CT(2) - CT(1) / beta) * num / den : CT(1) / beta;
+    const CT ir = CT(1) / rho;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const CT feq = E(q, rho);
+        const CT ds = kbc_shear<CT, USE_T, USE_Q>(q, m) - kbc_shear<CT, USE_T, USE_Q>(q, e);
+        const CT dh = f[q] - feq - ds;
+        f[q] -= beta * (CT(2) * ds + gamma * dh) - (CT(1) - beta) * force_src<CT>(q, ir, ux, uy, uz, fx, fy, fz) * feq;
+    }
+}
+
+template <class CT, int COL>
+__device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz, CT nu)
+{
+    if constexpr (COL == COL_CUM) collide_cum<CT>(f, rho, ux, uy, uz, nu);
+    else if constexpr (COL == COL_MRT) collide_mrt<CT>(f, rho, ux, uy, uz, nu);
+    else if constexpr (COL == COL_BGK) collide_bgk<CT>(f, rho, ux, uy, uz, fx, fy, fz, nu);
+    else {
+        constexpr bool central = COL >= COL_KBC_C1;
+        constexpr int v = central ? COL - COL_KBC_C1 + 1 : COL - COL_KBC_N1 + 1;
+        collide_kbc<CT, central, (v == 2 || v == 4), (v == 3 || v == 4)>(f, rho, ux, uy, uz, fx, fy, fz, nu);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Carreau-Yasuda local viscosity from the non-equilibrium second moments:
+// Pi = sum f (c-u)(c-u) - rho/3 I, S = -3/(2 rho tau) Pi, gamma_dot = sqrt(2 S:S),
+// nu = nu_inf + (nu0-nu_inf)(1 + (lambda gamma_dot)^a)^((n-1)/a), tau = 3 nu + 1/2, solved by
+// three Newton steps on g(tau) = tau - 3 nu_CY(K/tau) - 1/2 from tau = 3 nu0 + 1/2.
+// The viscosity law is the reference's (solver/lbm3d/core.h:763-766).
+// ---------------------------------------------------------------------------------------
+template <class CT>
+__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, CT nu_inf, CT nu0, CT lam, CT a, CT n, CT* S)
+{
+    CT Cxx = 0, Cyy = 0, Czz = 0, Cxy = 0, Cxz = 0, Cyz = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const CT dx = CT(cxq(q)) - ux, dy = CT(cyq(q)) - uy, dz = CT(czq(q)) - uz, v = f[q];
+        Cxx += dx * dx * v; Cyy += dy * dy * v; Czz += dz * dz * v;
+        Cxy += dx * dy * v; Cxz += dx * dz * v; Cyz += dy * dz * v;
+    }
+    const CT Pxx = Cxx - rho * CT(1.0 / 3.0), Pyy = Cyy - rho * CT(1.0 / 3.0), Pzz = Czz - rho * CT(1.0 / 3.0);
+    const CT pn = dsqrt<CT>(Pxx * Pxx + Pyy * Pyy + Pzz * Pzz + CT(2) * (Cxy * Cxy + Cxz * Cxz + Cyz * Cyz));
+    const CT K = CT(3) * CT(1.4142135623730951) * pn / (CT(2) * rho);
+    CT tau = CT(3) * nu0 + CT(0.5);
+    if (K > CT(0)) {
+        const CT e = (n - CT(1)) / a;
+#pragma unroll
+        for (int it = 0; it < 3; ++it) {
+            const CT g = K / tau;
+            const CT s = dpow<CT>(lam * g, a);
+            const CT p = dpow<CT>(CT(1) + s, e);
+            const CT nuc = nu_inf + (nu0 - nu_inf) * p;
+            const CT G = tau - CT(3) * nuc - CT(0.5);
+            const CT gdn = (nu0 - nu_inf) * (n - CT(1)) * s * p / (CT(1) + s);
+            const CT Gp = CT(1) + CT(3) * gdn / tau;
+            tau = tau - G / Gp;
+        }
+    }
+    const CT sc = CT(-3) / (CT(2) * rho * tau);
+    S[0] = sc * Pxx; S[1] = sc * Cxy; S[2] = sc * Cxz; S[3] = sc * Pyy; S[4] = sc * Cyz; S[5] = sc * Pzz;
+    return (tau - CT(0.5)) * CT(1.0 / 3.0);
+}
+
+} // namespace nnlbm

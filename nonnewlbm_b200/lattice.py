@@ -1,0 +1,180 @@
+"""Host-side lattice object over the C ABI (numpy in, numpy out).
+
+``Lattice`` is the Python face of the reference's policy composition (LBM_TYPE x
+STREAMING x MACRO x LBM_DATA x LBM_BC, solver/sim_tcpc/sim_tcpc.cu:431-438): a collision
+selector string, an equilibrium, a Carreau-Yasuda mode, a storage type and a label map.
+One ``Lattice`` owns one or more cases of a single library context.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi
+
+
+@dataclass
+class CaseSpec:
+    shape: tuple            # (nx, ny, nz)
+    collision: str = "CUM"
+    dtype: str = "f32"
+    equilibrium: str = "inv_cum_ref"
+    cy_mode: str = "none"
+    nu: float = 1.0 / 30.0
+    cy: tuple = (0.0, 0.0, 2.0, 1.0)   # nu0, lambda, a, n in lattice units
+    force: tuple = (0.0, 0.0, 0.0)
+    stats_f64: bool = True
+    storage_scale: float = 0.0
+
+    def desc(self) -> capi.CaseDesc:
+        nx, ny, nz = self.shape
+        col = self.collision.upper()
+        if col not in capi.COLLISIONS:
+            raise ValueError(f"unknown collision {self.collision!r}; choose one of {capi.COLLISIONS}")
+        return capi.CaseDesc(int(nx), int(ny), int(nz), capi.DTYPES[self.dtype.lower()], capi.COLLISIONS.index(col),
+                             capi.EQUILIBRIA[self.equilibrium.lower()], capi.CY_MODES[self.cy_mode.lower()],
+                             int(bool(self.stats_f64)), float(self.nu), float(self.cy[0]), float(self.cy[1]),
+                             float(self.cy[2]), float(self.cy[3]), float(self.force[0]), float(self.force[1]),
+                             float(self.force[2]), float(self.storage_scale))
+
+
+class Lattice:
+    """One library context holding ``len(specs)`` cases on CUDA device ``device``."""
+
+    def __init__(self, specs, device: int = 0):
+        if isinstance(specs, CaseSpec):
+            specs = [specs]
+        self.specs = list(specs)
+        arr = (capi.CaseDesc * len(self.specs))(*[s.desc() for s in self.specs])
+        h = ctypes.c_void_p()
+        rc = capi.lib().nnlbm_create(arr, len(self.specs), int(device), ctypes.byref(h))
+        self.h = h.value
+        if rc != capi.OK:
+            msg = capi.last_error(self.h) if self.h else "nnlbm_create failed"
+            self.close()
+            raise capi.NnlbmError(rc, msg)
+
+    # -- lifetime ---------------------------------------------------------------------
+    def close(self) -> None:
+        h = getattr(self, "h", None)
+        if h:
+            capi.lib().nnlbm_destroy(h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _chk(self, rc):
+        capi.check(self.h, rc)
+
+    def shape(self, ic: int = 0):
+        nx, ny, nz = self.specs[ic].shape
+        return (nz, ny, nx)
+
+    def ncells(self, ic: int = 0) -> int:
+        nx, ny, nz = self.specs[ic].shape
+        return nx * ny * nz
+
+    # -- set-up -------------------------------------------------------------------------
+    def set_map(self, labels: np.ndarray, ic: int = 0) -> None:
+        a = np.ascontiguousarray(labels, dtype=np.uint8).reshape(-1)
+        if a.size != self.ncells(ic):
+            raise ValueError(f"map has {a.size} cells, case {ic} has {self.ncells(ic)}")
+        self._chk(capi.lib().nnlbm_set_map(self.h, ic, a.ctypes.data))
+
+    def setup_tcpc(self, wall: np.ndarray, ic: int = 0) -> dict:
+        a = np.ascontiguousarray(wall, dtype=np.int32).reshape(-1)
+        if a.size != self.ncells(ic):
+            raise ValueError("wall array size does not match the lattice")
+        counts = np.zeros(10, dtype=np.int64)
+        self._chk(capi.lib().nnlbm_setup_tcpc(self.h, ic, a.ctypes.data, counts.ctypes.data))
+        keys = ["left_area", "right_area", "outlet5", "outlet6", "wall", "fluid", "vtk3", "vtk4", "vtk5", "vtk6"]
+        return dict(zip(keys, (int(v) for v in counts)))
+
+    def init_equilibrium(self, rho=1.0, ux=0.0, uy=0.0, uz=0.0, ic: int | None = None) -> None:
+        for k in self._cases(ic):
+            self._chk(capi.lib().nnlbm_init_equilibrium(self.h, k, rho, ux, uy, uz))
+
+    def set_inflow(self, ivc_flux=0.0, svc_flux=0.0, rho_left=1.0, rho_right=1.0, rho_eq=1.0, ic: int = 0) -> None:
+        self._chk(capi.lib().nnlbm_set_inflow(self.h, ic, ivc_flux, svc_flux, rho_left, rho_right, rho_eq))
+
+    def set_inflow_profile(self, u: np.ndarray, ic: int = 0) -> None:
+        a = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
+        self._chk(capi.lib().nnlbm_set_inflow_profile(self.h, ic, capi.dptr(a), a.shape[0]))
+
+    def set_schedule(self, rows: np.ndarray, ic: int = 0) -> None:
+        a = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 3)
+        self._chk(capi.lib().nnlbm_set_schedule(self.h, ic, capi.dptr(a), a.shape[0]))
+
+    # -- time stepping --------------------------------------------------------------------
+    def step(self, n: int = 1, stats: bool = False, macro: bool = False, reduce: bool = False) -> None:
+        flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0) | (capi.STEP_REDUCE if reduce else 0)
+        self._chk(capi.lib().nnlbm_step(self.h, int(n), flags))
+
+    def autotune(self) -> None:
+        self._chk(capi.lib().nnlbm_autotune(self.h))
+
+    def stat_reset(self, ic: int | None = None) -> None:
+        for k in self._cases(ic):
+            self._chk(capi.lib().nnlbm_stat_reset(self.h, k))
+
+    # -- results --------------------------------------------------------------------------
+    def macro(self, field: int, ic: int = 0) -> np.ndarray:
+        out = np.empty(self.ncells(ic))
+        self._chk(capi.lib().nnlbm_get_macro(self.h, ic, int(field), capi.dptr(out)))
+        return out.reshape(self.shape(ic))
+
+    def stats(self, ic: int = 0):
+        out = np.empty(6 * self.ncells(ic))
+        n = ctypes.c_int64()
+        self._chk(capi.lib().nnlbm_get_stats(self.h, ic, capi.dptr(out), ctypes.byref(n)))
+        return out.reshape((6,) + self.shape(ic)), int(n.value)
+
+    def export_df(self, ic: int = 0) -> np.ndarray:
+        out = np.empty(27 * self.ncells(ic))
+        self._chk(capi.lib().nnlbm_export_df(self.h, ic, capi.dptr(out)))
+        return out.reshape((27,) + self.shape(ic))
+
+    def import_df(self, df: np.ndarray, ic: int = 0) -> None:
+        a = np.ascontiguousarray(df, dtype=np.float64).reshape(-1)
+        if a.size != 27 * self.ncells(ic):
+            raise ValueError("population array size does not match the lattice")
+        self._chk(capi.lib().nnlbm_import_df(self.h, ic, capi.dptr(a)))
+
+    def reduce(self, ic: int = 0) -> np.ndarray:
+        out = np.zeros(5)
+        self._chk(capi.lib().nnlbm_reduce(self.h, ic, capi.dptr(out)))
+        return out
+
+    def step_info(self, ic: int = 0) -> dict:
+        fl, bc, la = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        by = ctypes.c_double()
+        self._chk(capi.lib().nnlbm_step_info(self.h, ic, ctypes.byref(fl), ctypes.byref(bc), ctypes.byref(la),
+                                             ctypes.byref(by)))
+        return {"fluid_cells": fl.value, "bc_cells": bc.value, "launches_per_step": la.value,
+                "bytes_per_step": by.value}
+
+    def profile_step(self, n: int, stats: bool = False, ic: int = 0) -> dict:
+        """Run n real steps as separate launches with CUDA events around each kernel; returns
+        the mean device milliseconds per launch of each kernel kind."""
+        ms = np.zeros(5)
+        cnt = np.zeros(5, dtype=np.int64)
+        self._chk(capi.lib().nnlbm_profile_step(self.h, ic, int(n), capi.STEP_STATS if stats else 0, capi.dptr(ms),
+                                                cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        names = ["bc_gather", "step", "bc_write", "refd_velocity", "refd_stress"]
+        return {k: (float(ms[i] / cnt[i]) if cnt[i] else 0.0, int(cnt[i])) for i, k in enumerate(names)}
+
+    @property
+    def stream(self) -> int:
+        return capi.lib().nnlbm_stream(self.h) or 0
+
+    def _cases(self, ic):
+        return range(len(self.specs)) if ic is None else [ic]

@@ -1,0 +1,198 @@
+"""Parity of the sm_100a step (through the C ABI) against the FP64 C oracle.
+
+Bars: FP64 storage matches the oracle to 1e-12 relative per population after 100 steps
+(dead populations excluded, see helpers.dead_mask); FP32/FP16/BF16 storage are checked
+against the FP64 oracle with the tolerances written in each test.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from nonnewlbm_b200 import CaseSpec, Lattice, capi
+from nonnewlbm_b200 import geometry as G
+
+from helpers import dead_mask, max_rel, small_junction
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+
+
+def _tcpc_pair(collision: int, dtype="f64", eq=O.EQ_INV_CUM_REF, nu=0.02, cy_mode=O.CY_NONE, cy=(0.0, 0.0, 2.0, 1.0),
+               ivc=0.03, svc=0.02):
+    wall = small_junction()
+    nz, ny, nx = wall.shape
+    orc = O.Oracle(nx, ny, nz, collision=collision, equilibrium=eq, nu=nu, cy_mode=cy_mode, cy=cy)
+    rc, counts = orc.setup_tcpc(wall)
+    assert rc == 0
+    eqname = {v: k for k, v in capi.EQUILIBRIA.items()}[eq]
+    cyname = {0: "none", 1: "ref-fd", 2: "local-neq"}[cy_mode]
+    lat = Lattice(CaseSpec((nx, ny, nz), collision=O.COLLISIONS[collision], dtype=dtype, equilibrium=eqname,
+                           cy_mode=cyname, nu=nu, cy=cy))
+    c2 = lat.setup_tcpc(wall)
+    assert c2["left_area"] == counts[0] and c2["outlet6"] == counts[3]
+    for L in (orc, lat):
+        L.set_inflow(ivc_flux=ivc * counts[0], svc_flux=svc * counts[1])
+        L.init_equilibrium()
+    return orc, lat
+
+
+@pytest.mark.parametrize("collision", range(11), ids=O.COLLISIONS)
+def test_fp64_tcpc_100_steps(collision):
+    orc, lat = _tcpc_pair(collision)
+    orc.step(100)
+    lat.step(100, macro=True)
+    labels = orc.get_map()
+    a, b = lat.export_df(), orc.get_df()
+    assert max_rel(a, b, dead_mask(labels)) <= FP64_TOL
+    for fo, fl in ((O.M_RHO, capi.M_RHO), (O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        assert np.max(np.abs(lat.macro(fl) - orc.get_macro(fo))) <= 1e-13
+
+
+def test_fp64_odd_step_count_and_layout():
+    """Odd and even step counts leave the two A-A layouts; both must export the same state."""
+    orc, lat = _tcpc_pair(O.COLLISIONS.index("CUM"))
+    labels = orc.get_map()
+    dead = dead_mask(labels)
+    for n in (1, 2, 3, 7):
+        orc.step(n)
+        lat.step(n)
+        assert max_rel(lat.export_df(), orc.get_df(), dead) <= FP64_TOL, n
+
+
+def test_fp64_import_export_roundtrip():
+    orc, lat = _tcpc_pair(0)
+    orc.step(5)
+    df = orc.get_df()
+    lat.import_df(df)
+    dead = dead_mask(orc.get_map())
+    assert max_rel(lat.export_df(), df, dead) == 0.0
+    orc.step(10)
+    lat.step(10)
+    assert max_rel(lat.export_df(), orc.get_df(), dead) <= FP64_TOL
+
+
+@pytest.mark.parametrize("eq", [O.EQ_INV_CUM, O.EQ_DEFAULT, O.EQ_ENTROPIC])
+def test_fp64_equilibria(eq):
+    orc, lat = _tcpc_pair(0, eq=eq)
+    orc.step(40)
+    lat.step(40)
+    assert max_rel(lat.export_df(), orc.get_df(), dead_mask(orc.get_map())) <= FP64_TOL
+
+
+def test_fp64_pipe_generic_bcs():
+    m, prof = G.pipe_map(24, 12, 12, 4.5)
+    nz, ny, nx = m.shape
+    orc = O.Oracle(nx, ny, nz, collision=0, nu=1.0 / 30.0)
+    lat = Lattice(CaseSpec((nx, ny, nz), collision="CUM", dtype="f64", nu=1.0 / 30.0))
+    orc.set_map(m)
+    orc.set_inflow_profile(G.expand_profile(m, prof) * 0.04)
+    lat.set_map(m)
+    lat.set_inflow_profile(prof * 0.04)
+    for L in (orc, lat):
+        L.init_equilibrium()
+    orc.step(100)
+    lat.step(100)
+    assert max_rel(lat.export_df(), orc.get_df(), dead_mask(m)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("collision", [0, 9, 10])
+def test_fp64_periodic_box(collision):
+    m, prof = G.dense_box_map(16, 10, 8)
+    nz, ny, nx = m.shape
+    orc = O.Oracle(nx, ny, nz, collision=collision, nu=0.05 / 3)
+    lat = Lattice(CaseSpec((nx, ny, nz), collision=O.COLLISIONS[collision], dtype="f64", nu=0.05 / 3))
+    orc.set_map(m)
+    orc.set_inflow_profile(G.expand_profile(m, prof) * 0.05)
+    lat.set_map(m)
+    lat.set_inflow_profile(prof * 0.05)
+    for L in (orc, lat):
+        L.init_equilibrium()
+    orc.step(100)
+    lat.step(100)
+    assert max_rel(lat.export_df(), orc.get_df()) <= FP64_TOL
+
+
+CY = (0.05, 40.0, 2.0, 0.3568)  # nu0, lambda, a, n in lattice units (nu_inf = 0.02)
+
+
+def test_fp64_cy_local_neq():
+    orc, lat = _tcpc_pair(0, cy_mode=O.CY_LOCAL_NEQ, cy=CY)
+    orc.step(100)
+    lat.step(100, macro=True)
+    assert max_rel(lat.export_df(), orc.get_df(), dead_mask(orc.get_map())) <= FP64_TOL
+    fluid = orc.get_map() == G.MAP_FLUID
+    s_o = orc.get_macro(O.M_S12)[fluid]
+    s_l = lat.macro(capi.M_S12)[fluid]
+    assert np.max(np.abs(s_o - s_l)) <= 1e-12 * max(1.0, np.max(np.abs(s_o)))
+
+
+def test_fp64_cy_ref_fd():
+    orc, lat = _tcpc_pair(0, cy_mode=O.CY_REF_FD, cy=CY)
+    orc.step(100)
+    lat.step(100, macro=True)
+    assert max_rel(lat.export_df(), orc.get_df(), dead_mask(orc.get_map())) <= FP64_TOL
+    # the force field is non-zero, so the three-phase path was exercised
+    assert np.max(np.abs(orc.get_macro(O.M_FX))) > 0
+
+
+def test_fp64_stats_and_reduce():
+    orc, lat = _tcpc_pair(0)
+    orc.step(30, accumulate_stats=False)
+    lat.step(30)
+    orc.step(20, accumulate_stats=True)
+    lat.step(20, stats=True, macro=True, reduce=True)
+    st, n = lat.stats()
+    assert n == 20
+    jx = orc.get_macro(O.M_VM_PLUS_X) + orc.get_macro(O.M_VM_MINUS_X)
+    assert np.max(np.abs(st[0] - jx)) <= 1e-12
+    assert np.max(np.abs(st[4] - orc.get_macro(O.M_VM_YY))) <= 1e-14
+    r_l, r_o = lat.reduce(), orc.reduce()
+    assert abs(r_l[0] - r_o[0]) <= 1e-9
+    assert np.max(np.abs(r_l[1:] - r_o[1:])) <= 1e-12
+
+
+@pytest.mark.parametrize("dtype,tol_u", [("f32", 2e-5), ("f16", 2e-3), ("bf16", 2e-2)])
+def test_reduced_precision_vs_fp64_oracle(dtype, tol_u):
+    """Velocity of FP32 / FP16 / BF16 storage against the FP64 oracle after 200 steps,
+    relative to the peak velocity."""
+    orc, lat = _tcpc_pair(0, dtype=dtype)
+    orc.step(200)
+    lat.step(200, macro=True)
+    fluid = orc.get_map() == G.MAP_FLUID
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
+    for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
+        assert err <= tol_u, (dtype, err)
+
+
+def test_autotune_keeps_state():
+    orc, lat = _tcpc_pair(0)
+    orc.step(4)
+    lat.step(4)
+    lat.autotune()
+    orc.step(6)
+    lat.step(6)
+    assert max_rel(lat.export_df(), orc.get_df(), dead_mask(orc.get_map())) <= FP64_TOL
+
+
+def test_batched_cases_match_single():
+    wall = small_junction()
+    nz, ny, nx = wall.shape
+    specs = [CaseSpec((nx, ny, nz), dtype="f64", nu=nu) for nu in (0.02, 0.05)]
+    lat = Lattice(specs)
+    singles = [Lattice(s) for s in specs]
+    for k in range(2):
+        lat.setup_tcpc(wall, ic=k)
+        singles[k].setup_tcpc(wall)
+        for L, ic in ((lat, k), (singles[k], 0)):
+            L.set_inflow(ivc_flux=5.0, svc_flux=3.0, ic=ic)
+    lat.init_equilibrium()
+    for s in singles:
+        s.init_equilibrium()
+        s.step(25)
+    lat.step(25)
+    for k in range(2):
+        assert np.array_equal(lat.export_df(k), singles[k].export_df())
