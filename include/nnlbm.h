@@ -123,6 +123,10 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map);
  * Returns NNLBM_ERR_AREA where the reference sets `terminate` (sim_tcpc.cu:633-640). */
 int nnlbm_setup_tcpc(nnlbm_ctx* ctx, int ic, const int32_t* wall, int64_t* counts);
 
+/* The same boundary setup without a context or a device (host only): map_out [nz][ny][nx]
+ * solver labels, counts as above. */
+int nnlbm_tcpc_labels(int32_t nx, int32_t ny, int32_t nz, const int32_t* wall, uint8_t* map_out, int64_t* counts);
+
 /* Replaces: resetLattice / setEqLat + LBMKernelInit (sim_tcpc.cu:647-655,
  * lbm.hpp:1-39, core.h:833-863). */
 int nnlbm_init_equilibrium(nnlbm_ctx* ctx, int ic, double rho, double ux, double uy, double uz);

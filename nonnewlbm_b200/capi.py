@@ -28,7 +28,7 @@ EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
     "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_stat_reset", "nnlbm_get_macro",
     "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_step_info", "nnlbm_profile_step",
-    "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy",
+    "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels",
 ]
 
 
@@ -84,6 +84,7 @@ def lib():
         L.nnlbm_stream.restype = _vp
         L.nnlbm_last_error.argtypes = [_vp, ctypes.c_char_p, ctypes.c_size_t]
         L.nnlbm_destroy.argtypes = [_vp]
+        L.nnlbm_tcpc_labels.argtypes = [ctypes.c_int32] * 3 + [_vp, _vp, _vp]
         _lib = L
     return _lib
 
@@ -101,3 +102,17 @@ def last_error(h) -> str:
 def check(h, rc: int) -> None:
     if rc != OK:
         raise NnlbmError(rc, last_error(h))
+
+
+def tcpc_labels(wall: np.ndarray):
+    """Host-only TCPC boundary setup (nnlbm_tcpc_labels): geometry wall array [z][y][x] ->
+    (solver map, counts dict, status)."""
+    w = np.ascontiguousarray(wall, dtype=np.int32)
+    nz, ny, nx = w.shape
+    m = np.zeros(w.shape, dtype=np.uint8)
+    counts = np.zeros(10, dtype=np.int64)
+    rc = lib().nnlbm_tcpc_labels(nx, ny, nz, w.ctypes.data, m.ctypes.data, counts.ctypes.data)
+    if rc not in (OK, ERR_AREA):
+        raise NnlbmError(rc, "invalid TCPC geometry")
+    keys = ["left_area", "right_area", "outlet5", "outlet6", "wall", "fluid", "vtk3", "vtk4", "vtk5", "vtk6"]
+    return m, dict(zip(keys, (int(v) for v in counts))), rc

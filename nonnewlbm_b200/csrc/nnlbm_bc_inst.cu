@@ -1,5 +1,5 @@
-// nnlbm_bc_inst.cu -- open-plane and CY_REF_FD phase kernels for one storage type
-// (NNLBM_DT), plus the initial-state fill.
+// nnlbm_bc_inst.cu -- the open-plane gather, the CY_REF_FD phase kernels and the
+// initial-state fills for one storage type (NNLBM_DT).
 #include "nnlbm_kernels.cuh"
 
 #ifndef NNLBM_DT
@@ -13,24 +13,23 @@ namespace nnlbm {
 
 // every slot q of every cell <- feq_q(rho, u): a uniform state is valid in either A-A layout
 template <int DT>
-__global__ void k_fill_eq(const KArgs<typename Storage<DT>::CT> a, typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
+__global__ void k_fill_eq(const CaseArgs<typename Storage<DT>::CT> a, typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
                           typename Storage<DT>::CT uy, typename Storage<DT>::CT uz)
 {
     using S = Storage<DT>;
     using CT = typename S::CT;
-    using T = typename S::T;
     CT f[27];
     equilibrium<CT>(a.eq, rho, ux, uy, uz, f);
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.N; c += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
-        for (int q = 0; q < 27; ++q) S::store((T*)a.dfq[q], c, q, f[q], a.scale);
+        for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, q), (int)c, q, f[q], a.scale);
     }
 }
 
 // initial macro state (LBMKernelInit, core.h:833-863): rho/u from f at FLUID and PERIODIC
 // cells, rho = 1 and u = 0 elsewhere, F = the homogeneous force, S = 0
 template <int DT>
-__global__ void k_init_macro(const KArgs<typename Storage<DT>::CT> a, typename Storage<DT>::CT rho0, typename Storage<DT>::CT ux0,
+__global__ void k_init_macro(const CaseArgs<typename Storage<DT>::CT> a, typename Storage<DT>::CT rho0, typename Storage<DT>::CT ux0,
                              typename Storage<DT>::CT uy0, typename Storage<DT>::CT uz0)
 {
     using CT = typename Storage<DT>::CT;
@@ -39,7 +38,7 @@ __global__ void k_init_macro(const KArgs<typename Storage<DT>::CT> a, typename S
     CT r, u, v, w;
     density_velocity<CT>(f, a.fx, a.fy, a.fz, r, u, v, w);
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.N; c += (int64_t)gridDim.x * blockDim.x) {
-        const int lab = a.label[c];
+        const int lab = a.label[c] & L_MASK;
         const bool fl = lab == L_FLUID || lab == L_PERIODIC;
         CT* M = a.macro;
         M[M_RHO * a.N + c] = fl ? r : CT(1);
@@ -54,43 +53,35 @@ __global__ void k_init_macro(const KArgs<typename Storage<DT>::CT> a, typename S
 void NNLBM_CAT(launch_bc_gather_, NNLBM_DT)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<NNLBM_DT>::CT;
-    const KArgs<CT>& a = *(const KArgs<CT>*)args;
-    if (odd) k_bc_gather<NNLBM_DT, true><<<grid, block, 0, s>>>(a);
-    else k_bc_gather<NNLBM_DT, false><<<grid, block, 0, s>>>(a);
-}
-
-void NNLBM_CAT(launch_bc_write_, NNLBM_DT)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args)
-{
-    using CT = typename Storage<NNLBM_DT>::CT;
-    const KArgs<CT>& a = *(const KArgs<CT>*)args;
-    if (odd) k_bc_write<NNLBM_DT, true><<<grid, block, 0, s>>>(a);
-    else k_bc_write<NNLBM_DT, false><<<grid, block, 0, s>>>(a);
+    const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
+    if (odd) k_bc_gather<NNLBM_DT, true><<<grid, block, 0, s>>>(g);
+    else k_bc_gather<NNLBM_DT, false><<<grid, block, 0, s>>>(g);
 }
 
 void NNLBM_CAT(launch_refd_velocity_, NNLBM_DT)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<NNLBM_DT>::CT;
-    const KArgs<CT>& a = *(const KArgs<CT>*)args;
-    if (odd) k_refd_velocity<NNLBM_DT, true><<<grid, block, 0, s>>>(a);
-    else k_refd_velocity<NNLBM_DT, false><<<grid, block, 0, s>>>(a);
+    const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
+    if (odd) k_refd_velocity<NNLBM_DT, true><<<grid, block, 0, s>>>(g);
+    else k_refd_velocity<NNLBM_DT, false><<<grid, block, 0, s>>>(g);
 }
 
 void NNLBM_CAT(launch_refd_stress_, NNLBM_DT)(bool, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<NNLBM_DT>::CT;
-    k_refd_stress<CT><<<grid, block, 0, s>>>(*(const KArgs<CT>*)args);
+    k_refd_stress<CT><<<grid, block, 0, s>>>(*(const GroupArgs<CT>*)args);
 }
 
 void NNLBM_CAT(launch_fill_eq_, NNLBM_DT)(const void* args, double rho, double ux, double uy, double uz, cudaStream_t s)
 {
     using CT = typename Storage<NNLBM_DT>::CT;
-    k_fill_eq<NNLBM_DT><<<148 * 8, 256, 0, s>>>(*(const KArgs<CT>*)args, (CT)rho, (CT)ux, (CT)uy, (CT)uz);
+    k_fill_eq<NNLBM_DT><<<148 * 8, 256, 0, s>>>(*(const CaseArgs<CT>*)args, (CT)rho, (CT)ux, (CT)uy, (CT)uz);
 }
 
 void NNLBM_CAT(launch_init_macro_, NNLBM_DT)(const void* args, double rho, double ux, double uy, double uz, cudaStream_t s)
 {
     using CT = typename Storage<NNLBM_DT>::CT;
-    k_init_macro<NNLBM_DT><<<148 * 8, 256, 0, s>>>(*(const KArgs<CT>*)args, (CT)rho, (CT)ux, (CT)uy, (CT)uz);
+    k_init_macro<NNLBM_DT><<<148 * 8, 256, 0, s>>>(*(const CaseArgs<CT>*)args, (CT)rho, (CT)ux, (CT)uy, (CT)uz);
 }
 
 } // namespace nnlbm

@@ -1,5 +1,6 @@
 // nnlbm_capi.cu -- the C ABI of libnnlbm.so (declared in include/nnlbm.h): contexts, device
-// buffers, the TCPC boundary setup, the per-step launch sequence and its CUDA graph.
+// buffers, the TCPC boundary setup, the packed work lists, the per-step launch sequence of
+// each launch group and its CUDA graphs.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -22,36 +23,35 @@ namespace nnlbm {
     NNLBM_DECL_STEP(DT, 5) NNLBM_DECL_STEP(DT, 6) NNLBM_DECL_STEP(DT, 7) NNLBM_DECL_STEP(DT, 8) NNLBM_DECL_STEP(DT, 9) \
     NNLBM_DECL_STEP(DT, 10)
 NNLBM_DECL_STEP_DT(0) NNLBM_DECL_STEP_DT(1) NNLBM_DECL_STEP_DT(2) NNLBM_DECL_STEP_DT(3)
-#define NNLBM_DECL_BC(DT)                                                                \
-    void launch_bc_gather_##DT(bool, dim3, dim3, cudaStream_t, const void*);            \
-    void launch_bc_write_##DT(bool, dim3, dim3, cudaStream_t, const void*);             \
-    void launch_refd_velocity_##DT(bool, dim3, dim3, cudaStream_t, const void*);        \
-    void launch_refd_stress_##DT(bool, dim3, dim3, cudaStream_t, const void*);          \
+#define NNLBM_DECL_AUX(DT)                                                                \
+    void launch_bc_gather_##DT(bool, dim3, dim3, cudaStream_t, const void*);             \
+    void launch_refd_velocity_##DT(bool, dim3, dim3, cudaStream_t, const void*);         \
+    void launch_refd_stress_##DT(bool, dim3, dim3, cudaStream_t, const void*);           \
     void launch_fill_eq_##DT(const void*, double, double, double, double, cudaStream_t); \
     void launch_init_macro_##DT(const void*, double, double, double, double, cudaStream_t);
-NNLBM_DECL_BC(0) NNLBM_DECL_BC(1) NNLBM_DECL_BC(2) NNLBM_DECL_BC(3)
+NNLBM_DECL_AUX(0) NNLBM_DECL_AUX(1) NNLBM_DECL_AUX(2) NNLBM_DECL_AUX(3)
 
-StepLauncher step_launcher(int dt, int col)
+GroupLauncher step_launcher(int dt, int col)
 {
 #define NNLBM_ROW(DT)                                                                                     \
     {launch_step_##DT##_0, launch_step_##DT##_1, launch_step_##DT##_2, launch_step_##DT##_3,             \
      launch_step_##DT##_4, launch_step_##DT##_5, launch_step_##DT##_6, launch_step_##DT##_7,             \
      launch_step_##DT##_8, launch_step_##DT##_9, launch_step_##DT##_10}
-    static const StepLauncher table[4][11] = {NNLBM_ROW(0), NNLBM_ROW(1), NNLBM_ROW(2), NNLBM_ROW(3)};
+    static const GroupLauncher table[4][11] = {NNLBM_ROW(0), NNLBM_ROW(1), NNLBM_ROW(2), NNLBM_ROW(3)};
     return table[dt][col];
 }
 
-struct BcLaunchers {
-    StepLauncher gather, write, refd_velocity, refd_stress;
+struct AuxLaunchers {
+    GroupLauncher gather, refd_velocity, refd_stress;
     void (*fill_eq)(const void*, double, double, double, double, cudaStream_t);
     void (*init_macro)(const void*, double, double, double, double, cudaStream_t);
 };
-static const BcLaunchers& bc_launchers(int dt)
+static const AuxLaunchers& aux_launchers(int dt)
 {
-#define NNLBM_BCROW(DT)                                                                                      \
-    {launch_bc_gather_##DT, launch_bc_write_##DT, launch_refd_velocity_##DT, launch_refd_stress_##DT,      \
-     launch_fill_eq_##DT, launch_init_macro_##DT}
-    static const BcLaunchers t[4] = {NNLBM_BCROW(0), NNLBM_BCROW(1), NNLBM_BCROW(2), NNLBM_BCROW(3)};
+#define NNLBM_AUXROW(DT)                                                                                   \
+    {launch_bc_gather_##DT, launch_refd_velocity_##DT, launch_refd_stress_##DT, launch_fill_eq_##DT,     \
+     launch_init_macro_##DT}
+    static const AuxLaunchers t[4] = {NNLBM_AUXROW(0), NNLBM_AUXROW(1), NNLBM_AUXROW(2), NNLBM_AUXROW(3)};
     return t[dt];
 }
 } // namespace nnlbm
@@ -61,41 +61,59 @@ using namespace nnlbm;
 namespace {
 
 const int kStorageBytes[4] = {8, 4, 2, 2};
+const int kChunk = 32;
 
 struct Case {
     nnlbm_case_desc d{};
     int64_t N = 0;
     int ct_bytes = 4;        // arithmetic type size (8 for F64 storage)
     double scale = 1.0;      // 16-bit storage scale
+    int group = 0;
     // device buffers
     void* df = nullptr;      // 27 direction arrays
     size_t q_stride = 0;     // elements between direction arrays
     uint8_t* d_label = nullptr;
-    int32_t* d_bc_cell = nullptr;
-    void* d_bc_prof = nullptr;
-    void* d_bc_buf = nullptr;
     void* d_macro = nullptr;
     void* d_stats = nullptr;
     void* d_ctl = nullptr;
     int64_t ctl_cap = 0;
-    int* d_ints = nullptr;   // cursor, done, err
     double* d_red = nullptr;
+    int* d_err = nullptr;
     // host state
-    std::vector<uint8_t> label;
-    std::vector<int32_t> bc_cell;
-    std::vector<double> bc_prof;     // [n_bc][3]
-    int64_t n_fluid = 0, left_area = 0, right_area = 0, n_inflow_eq = 0;
+    std::vector<uint8_t> label;      // plain solver labels
+    std::vector<uint8_t> dlabel;     // labels with the work flags of the device copy
+    std::vector<int4> chunks;        // {first cell, y | z << 16, 0, first self index}
+    std::vector<int32_t> self_cell;  // cells handled by their own thread, in cell order
+    std::vector<int32_t> gather_self;// self indices of the gathered nodes
+    std::vector<double> self_prof;   // [n_self][3] prescribed velocity of INFLOW_EQ nodes
+    int64_t n_fluid = 0, n_bc = 0, left_area = 0, right_area = 0, n_inflow_eq = 0;
     double ivc_flux = 0, svc_flux = 0, rho_left = 1, rho_right = 1, rho_eq = 1;
     std::vector<double> sched;       // rows of {ivc_flux, svc_flux, profile_scale}
     int64_t parity = 0;              // steps done since the layout was last reset, mod 2
     int64_t iterations = 0;
     int64_t n_stats = 0;
     bool has_map = false, has_state = false;
-    int bx = 64, by = 4;
-    // one captured step per A-A parity
+    std::vector<char> args;          // CaseArgs<CT>
+};
+
+struct Group {
+    int dtype = 1, collision = 0;
+    std::vector<int> cases;          // context case indices
+    bool dirty = true;
+    void* d_cases = nullptr;         // CaseArgs<CT>[n]
+    int4* d_chunks = nullptr;
+    int n_chunks = 0;
+    int4* d_gather = nullptr;
+    int n_gather = 0;
+    void* d_bc_prof = nullptr;
+    void* d_bc_buf = nullptr;
+    int64_t n_self = 0;
+    int* d_ints = nullptr;           // cursor, done
+    bool any_refd = false;
+    int block = 256;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_gen = ~0ull, gen = 0;
-    std::vector<char> args;          // KArgs<CT>
+    std::vector<char> args;          // GroupArgs<CT>
 };
 
 } // namespace
@@ -104,6 +122,7 @@ struct nnlbm_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::vector<Case> cases;
+    std::vector<Group> groups;
     std::string err;
 };
 
@@ -129,11 +148,11 @@ int set_err(nnlbm_ctx* ctx, int code, const char* fmt, ...)
     } while (0)
 
 template <class CT>
-void fill_args(Case& c, KArgs<CT>& a)
+void fill_case_args(const Case& c, CaseArgs<CT>& a)
 {
     memset(&a, 0, sizeof a);
-    const size_t eb = kStorageBytes[c.d.dtype];
-    for (int q = 0; q < 27; ++q) a.dfq[q] = (char*)c.df + (size_t)q * c.q_stride * eb;
+    a.df = c.df;
+    a.qstride = (int64_t)c.q_stride;
     a.label = c.d_label;
     a.nx = c.d.nx; a.ny = c.d.ny; a.nz = c.d.nz;
     a.N = c.N;
@@ -144,22 +163,20 @@ void fill_args(Case& c, KArgs<CT>& a)
     a.macro = (CT*)c.d_macro;
     a.stats = c.d_stats; a.stats_f64 = c.d.stats_f64;
     a.ctl = (const StepCtl<CT>*)c.d_ctl;
-    a.cursor = c.d_ints; a.done = c.d_ints + 1; a.err = c.d_ints + 2;
     a.red = c.d_red;
-    a.bc_cell = c.d_bc_cell; a.bc_prof = (const CT*)c.d_bc_prof; a.bc_buf = (CT*)c.d_bc_buf;
-    a.n_bc = (int)c.bc_cell.size();
+    a.err = c.d_err;
 }
 
-void rebuild_args(Case& c)
+void rebuild_case_args(nnlbm_ctx* ctx, Case& c)
 {
     if (c.ct_bytes == 8) {
-        c.args.resize(sizeof(KArgs<double>));
-        fill_args<double>(c, *(KArgs<double>*)c.args.data());
+        c.args.resize(sizeof(CaseArgs<double>));
+        fill_case_args<double>(c, *(CaseArgs<double>*)c.args.data());
     } else {
-        c.args.resize(sizeof(KArgs<float>));
-        fill_args<float>(c, *(KArgs<float>*)c.args.data());
+        c.args.resize(sizeof(CaseArgs<float>));
+        fill_case_args<float>(c, *(CaseArgs<float>*)c.args.data());
     }
-    c.gen++;
+    ctx->groups[c.group].dirty = true;
 }
 
 int check_case(nnlbm_ctx* ctx, int ic)
@@ -169,29 +186,12 @@ int check_case(nnlbm_ctx* ctx, int ic)
     return NNLBM_OK;
 }
 
-// upload a host vector of doubles to a device array of the case's arithmetic type
-int upload_ct(nnlbm_ctx* ctx, Case& c, void** dptr, const std::vector<double>& v)
-{
-    if (*dptr) { cudaFree(*dptr); *dptr = nullptr; }
-    size_t n = std::max<size_t>(v.size(), 1);
-    CK(cudaMalloc(dptr, n * c.ct_bytes));
-    if (!v.empty()) {
-        if (c.ct_bytes == 8) {
-            CK(cudaMemcpy(*dptr, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
-        } else {
-            std::vector<float> f(v.begin(), v.end());
-            CK(cudaMemcpy(*dptr, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
-        }
-    }
-    return NNLBM_OK;
-}
-
 int ensure_macro(nnlbm_ctx* ctx, Case& c)
 {
     if (c.d_macro) return NNLBM_OK;
     CK(cudaMalloc(&c.d_macro, (size_t)M_N * c.N * c.ct_bytes));
-    rebuild_args(c);
-    bc_launchers(c.d.dtype).init_macro(c.args.data(), 1.0, 0.0, 0.0, 0.0, ctx->stream);
+    rebuild_case_args(ctx, c);
+    aux_launchers(c.d.dtype).init_macro(c.args.data(), 1.0, 0.0, 0.0, 0.0, ctx->stream);
     CK(cudaGetLastError());
     return NNLBM_OK;
 }
@@ -203,7 +203,7 @@ int ensure_stats(nnlbm_ctx* ctx, Case& c)
     CK(cudaMalloc(&c.d_stats, bytes));
     CK(cudaMemsetAsync(c.d_stats, 0, bytes, ctx->stream));
     c.n_stats = 0;
-    rebuild_args(c);
+    rebuild_case_args(ctx, c);
     return NNLBM_OK;
 }
 
@@ -216,12 +216,12 @@ int ensure_ctl(nnlbm_ctx* ctx, Case& c, int64_t n)
     const size_t row = c.ct_bytes == 8 ? sizeof(StepCtl<double>) : sizeof(StepCtl<float>);
     CK(cudaMalloc(&c.d_ctl, cap * row));
     c.ctl_cap = cap;
-    rebuild_args(c);
+    rebuild_case_args(ctx, c);
     return NNLBM_OK;
 }
 
 template <class CT>
-void fill_ctl(Case& c, std::vector<char>& buf, int64_t n, int flags)
+void fill_ctl(const Case& c, std::vector<char>& buf, int64_t n, int flags)
 {
     buf.resize(n * sizeof(StepCtl<CT>));
     StepCtl<CT>* r = (StepCtl<CT>*)buf.data();
@@ -237,92 +237,193 @@ void fill_ctl(Case& c, std::vector<char>& buf, int64_t n, int flags)
         r[k].flags = f;
         r[k].pad = 0;
         // LBM_Data_Tcpc::inflowCondition{Left,Right} (sim_tcpc.cu:295-309) with
-        // inflow_right = -svc_flux (sim_tcpc.cu:660)
-        r[k].u_left = (CT)(c.left_area > 0 ? (CT)ivc / (CT)c.left_area : 0);
-        r[k].u_right = (CT)(c.right_area > 0 ? (CT)(-svc) / (CT)c.right_area : 0);
+        // inflow_right = -svc_flux (sim_tcpc.cu:660), divided in the arithmetic type
+        r[k].u_left = c.left_area > 0 ? (CT)ivc / (CT)c.left_area : CT(0);
+        r[k].u_right = c.right_area > 0 ? (CT)(-svc) / (CT)c.right_area : CT(0);
         r[k].rho_left = (CT)c.rho_left; r[k].rho_right = (CT)c.rho_right; r[k].rho_eq = (CT)c.rho_eq;
         r[k].prof_scale = (CT)ps;
     }
 }
 
-// enqueue one step (no host synchronisation); `odd` is the A-A parity of this step
-int enqueue_step(nnlbm_ctx* ctx, Case& c, bool odd)
+template <class CT>
+int upload_group(nnlbm_ctx* ctx, Group& g)
 {
-    const BcLaunchers& B = bc_launchers(c.d.dtype);
-    const dim3 blk(c.bx, c.by, 1);
-    const dim3 grd((c.d.nx + c.bx - 1) / c.bx, (c.d.ny + c.by - 1) / c.by, c.d.nz);
-    const int nbc = (int)c.bc_cell.size();
-    const dim3 bgrd((std::max(nbc, 1) + 127) / 128), bblk(128);
-    if (c.d.cy_mode == NNLBM_CY_REF_FD) {
-        B.refd_velocity(odd, grd, blk, ctx->stream, c.args.data());
-        B.refd_stress(odd, grd, blk, ctx->stream, c.args.data());
+    // per-case argument array and the concatenated work lists of the group
+    std::vector<CaseArgs<CT>> ca;
+    std::vector<int4> chunks, gather;
+    std::vector<CT> prof;
+    int64_t self_off = 0;
+    g.any_refd = false;
+    for (size_t j = 0; j < g.cases.size(); ++j) {
+        const Case& c = ctx->cases[g.cases[j]];
+        ca.push_back(*(const CaseArgs<CT>*)c.args.data());
+        g.any_refd |= c.d.cy_mode == NNLBM_CY_REF_FD;
+        for (int4 ch : c.chunks) {
+            ch.z = (int)j;
+            ch.w += (int)self_off;
+            chunks.push_back(ch);
+        }
+        for (int32_t k : c.gather_self) gather.push_back(make_int4(c.self_cell[k], (int)j, (int)(self_off + k), 0));
+        for (double v : c.self_prof) prof.push_back((CT)v);
+        self_off += (int64_t)c.self_cell.size();
     }
-    B.gather(odd, bgrd, bblk, ctx->stream, c.args.data());
-    step_launcher(c.d.dtype, c.d.collision)(odd, grd, blk, ctx->stream, c.args.data());
-    B.write(odd, bgrd, bblk, ctx->stream, c.args.data());
+    if (g.d_cases) cudaFree(g.d_cases);
+    if (g.d_chunks) cudaFree(g.d_chunks);
+    if (g.d_gather) cudaFree(g.d_gather);
+    if (g.d_bc_prof) cudaFree(g.d_bc_prof);
+    if (g.d_bc_buf) cudaFree(g.d_bc_buf);
+    g.d_cases = nullptr; g.d_chunks = nullptr; g.d_gather = nullptr; g.d_bc_prof = nullptr; g.d_bc_buf = nullptr;
+    CK(cudaMalloc(&g.d_cases, std::max<size_t>(ca.size(), 1) * sizeof(CaseArgs<CT>)));
+    CK(cudaMemcpy(g.d_cases, ca.data(), ca.size() * sizeof(CaseArgs<CT>), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void**)&g.d_chunks, std::max<size_t>(chunks.size(), 1) * sizeof(int4)));
+    if (!chunks.empty()) CK(cudaMemcpy(g.d_chunks, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void**)&g.d_gather, std::max<size_t>(gather.size(), 1) * sizeof(int4)));
+    if (!gather.empty()) CK(cudaMemcpy(g.d_gather, gather.data(), gather.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g.d_bc_prof, std::max<size_t>(prof.size(), 1) * sizeof(CT)));
+    if (!prof.empty()) CK(cudaMemcpy(g.d_bc_prof, prof.data(), prof.size() * sizeof(CT), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g.d_bc_buf, std::max<int64_t>(self_off, 1) * 4 * sizeof(CT)));
+    CK(cudaMemset(g.d_bc_buf, 0, std::max<int64_t>(self_off, 1) * 4 * sizeof(CT)));
+    g.n_chunks = (int)chunks.size();
+    g.n_gather = (int)gather.size();
+    g.n_self = self_off;
+    g.args.resize(sizeof(GroupArgs<CT>));
+    GroupArgs<CT>& ga = *(GroupArgs<CT>*)g.args.data();
+    memset(&ga, 0, sizeof ga);
+    ga.cases = (const CaseArgs<CT>*)g.d_cases;
+    ga.chunks = g.d_chunks;
+    ga.n_chunks = g.n_chunks;
+    ga.gather = g.d_gather;
+    ga.n_gather = g.n_gather;
+    ga.bc_prof = (const CT*)g.d_bc_prof;
+    ga.bc_buf = (CT*)g.d_bc_buf;
+    ga.cursor = g.d_ints;
+    ga.done = g.d_ints + 1;
+    g.dirty = false;
+    g.gen++;
+    return NNLBM_OK;
+}
+
+int prepare_group(nnlbm_ctx* ctx, Group& g)
+{
+    if (!g.dirty) return NNLBM_OK;
+    return g.dtype == NNLBM_F64 ? upload_group<double>(ctx, g) : upload_group<float>(ctx, g);
+}
+
+// enqueue one step of a group (no host synchronisation); `odd` is the A-A parity
+int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
+{
+    const AuxLaunchers& A = aux_launchers(g.dtype);
+    const int per_block = g.block / kChunk;
+    const dim3 cgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block), cblk(g.block);
+    if (g.any_refd) {
+        A.refd_velocity(odd, cgrid, cblk, ctx->stream, g.args.data());
+        A.refd_stress(odd, cgrid, cblk, ctx->stream, g.args.data());
+    }
+    if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 127) / 128), dim3(128), ctx->stream, g.args.data());
+    step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, g.args.data());
     CK(cudaGetLastError());
     return NNLBM_OK;
 }
 
-int ensure_graphs(nnlbm_ctx* ctx, Case& c)
+int ensure_graphs(nnlbm_ctx* ctx, Group& g)
 {
-    if (c.graph[0] && c.graph[1] && c.graph_gen == c.gen) return NNLBM_OK;
+    if (g.graph[0] && g.graph[1] && g.graph_gen == g.gen) return NNLBM_OK;
     for (int p = 0; p < 2; ++p) {
-        if (c.graph[p]) { cudaGraphExecDestroy(c.graph[p]); c.graph[p] = nullptr; }
-        cudaGraph_t g = nullptr;
+        if (g.graph[p]) { cudaGraphExecDestroy(g.graph[p]); g.graph[p] = nullptr; }
+        cudaGraph_t gr = nullptr;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_step(ctx, c, p == 1);
-        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-        if (rc != NNLBM_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        int rc = enqueue_step(ctx, g, p == 1);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &gr);
+        if (rc != NNLBM_OK) { if (gr) cudaGraphDestroy(gr); return rc; }
         if (e != cudaSuccess) return set_err(ctx, NNLBM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&c.graph[p], g, 0);
-        cudaGraphDestroy(g);
+        e = cudaGraphInstantiate(&g.graph[p], gr, 0);
+        cudaGraphDestroy(gr);
         if (e != cudaSuccess) return set_err(ctx, NNLBM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     }
-    c.graph_gen = c.gen;
+    g.graph_gen = g.gen;
     return NNLBM_OK;
 }
 
-int run_case_steps(nnlbm_ctx* ctx, Case& c, int64_t n, int flags, bool use_graph)
+// host side of one nnlbm_step call for every case of a group, up to the launches
+int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags)
 {
     int rc;
-    if ((flags & NNLBM_STEP_MACRO) || c.d.cy_mode == NNLBM_CY_REF_FD) {
-        if ((rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
+    int64_t parity = -1;
+    for (int ic : g.cases) {
+        Case& c = ctx->cases[ic];
+        if (!c.has_map || !c.has_state) return set_err(ctx, NNLBM_ERR_ARG, "case %d has no map or initial state", ic);
+        if (parity >= 0 && c.parity != parity)
+            return set_err(ctx, NNLBM_ERR_ARG, "cases of one launch group are at different step parities "
+                           "(re-initialise or re-import all of them)");
+        parity = c.parity;
+        if ((flags & NNLBM_STEP_MACRO) || c.d.cy_mode == NNLBM_CY_REF_FD)
+            if ((rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
+        if (flags & NNLBM_STEP_STATS)
+            if ((rc = ensure_stats(ctx, c)) != NNLBM_OK) return rc;
+        if ((rc = ensure_ctl(ctx, c, n)) != NNLBM_OK) return rc;
+        std::vector<char> buf;
+        if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n, flags);
+        else fill_ctl<float>(c, buf, n, flags);
+        CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
+        if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
     }
-    if (flags & NNLBM_STEP_STATS) {
-        if ((rc = ensure_stats(ctx, c)) != NNLBM_OK) return rc;
-    }
-    if ((rc = ensure_ctl(ctx, c, n)) != NNLBM_OK) return rc;
-    std::vector<char> buf;
-    if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n, flags);
-    else fill_ctl<float>(c, buf, n, flags);
-    CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemsetAsync(c.d_ints, 0, 2 * sizeof(int), ctx->stream)); // cursor, done
-    if (use_graph && (rc = ensure_graphs(ctx, c)) != NNLBM_OK) return rc;
-    for (int64_t k = 0; k < n; ++k) {
-        const int p = (int)((c.parity + k) & 1);
-        if (use_graph) CK(cudaGraphLaunch(c.graph[p], ctx->stream));
-        else if ((rc = enqueue_step(ctx, c, p == 1)) != NNLBM_OK) return rc;
-    }
-    c.parity = (c.parity + n) & 1;
-    c.iterations += n;
-    if (flags & NNLBM_STEP_STATS) c.n_stats += n;
+    if ((rc = prepare_group(ctx, g)) != NNLBM_OK) return rc;
+    CK(cudaMemsetAsync(g.d_ints, 0, 2 * sizeof(int), ctx->stream));
     return NNLBM_OK;
 }
 
-bool is_bc(int lab) { return lab >= L_IN_L && lab <= L_OUT_REQ; }
+void finish_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags)
+{
+    for (int ic : g.cases) {
+        Case& c = ctx->cases[ic];
+        c.parity = (c.parity + n) & 1;
+        c.iterations += n;
+        if (flags & NNLBM_STEP_STATS) c.n_stats += n;
+    }
+}
+
+int run_group_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool use_graph)
+{
+    int rc = prepare_steps(ctx, g, n, flags);
+    if (rc) return rc;
+    if (use_graph && (rc = ensure_graphs(ctx, g)) != NNLBM_OK) return rc;
+    const int64_t parity = ctx->cases[g.cases[0]].parity;
+    for (int64_t k = 0; k < n; ++k) {
+        const int p = (int)((parity + k) & 1);
+        if (use_graph) CK(cudaGraphLaunch(g.graph[p], ctx->stream));
+        else if ((rc = enqueue_step(ctx, g, p == 1)) != NNLBM_OK) return rc;
+    }
+    finish_steps(ctx, g, n, flags);
+    return NNLBM_OK;
+}
+
+int wait_and_check(nnlbm_ctx* ctx, int64_t n)
+{
+    std::vector<int> cur(ctx->groups.size() * 2), err(ctx->cases.size());
+    for (size_t i = 0; i < ctx->groups.size(); ++i)
+        CK(cudaMemcpyAsync(&cur[2 * i], ctx->groups[i].d_ints, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    for (size_t i = 0; i < ctx->cases.size(); ++i)
+        CK(cudaMemcpyAsync(&err[i], ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < ctx->groups.size(); ++i)
+        if (cur[2 * i] != n)
+            return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", i, cur[2 * i], (long long)n);
+    for (size_t i = 0; i < ctx->cases.size(); ++i)
+        if (err[i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
+    return NNLBM_OK;
+}
+
+bool is_pull_bc(int lab) { return lab == L_IN_L || lab == L_IN_R || lab == L_OUT_F || lab == L_OUT_B || lab == L_OUT_REQ; }
 
 // storage element <-> double on the host
 double decode(const Case& c, const void* base, size_t i, int q)
 {
-    const double w = q == 13 ? 8.0 / 27.0 : (nnzq(q) == 1 ? 2.0 / 27.0 : (nnzq(q) == 2 ? 1.0 / 54.0 : 1.0 / 216.0));
     switch (c.d.dtype) {
     case NNLBM_F64: return ((const double*)base)[i];
     case NNLBM_F32: return (double)(weight<float>(q) + ((const float*)base)[i]);
     case NNLBM_F16: return (double)(weight<float>(q) + __half2float(((const __half*)base)[i]) * (float)(1.0 / c.scale));
     default: return (double)(weight<float>(q) + __bfloat162float(((const __nv_bfloat16*)base)[i]) * (float)(1.0 / c.scale));
     }
-    (void)w;
 }
 
 void encode(const Case& c, void* base, size_t i, int q, double v)
@@ -358,71 +459,63 @@ extern "C" {
 int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx** out)
 {
     if (!desc || n_cases < 1 || !out) return NNLBM_ERR_ARG;
-    *out = nullptr;
     nnlbm_ctx* ctx = new nnlbm_ctx();
+    *out = ctx; // on failure the context carries the message; the caller destroys it
     ctx->device = device;
-    auto fail = [&](int rc) { nnlbm_destroy(ctx); return rc; };
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
-        // the context is returned so that the caller can read the message
-        set_err(ctx, NNLBM_ERR_CUDA, "no CUDA device %d (found %d)", device, ndev);
-        *out = ctx;
-        return NNLBM_ERR_CUDA;
+        cudaGetLastError();
+        return set_err(ctx, NNLBM_ERR_CUDA, "no CUDA device %d (found %d)", device, ndev);
     }
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        set_err(ctx, NNLBM_ERR_CUDA, "cannot initialise device %d", device);
-        *out = ctx;
-        return NNLBM_ERR_CUDA;
-    }
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return set_err(ctx, NNLBM_ERR_CUDA, "cannot initialise device %d", device);
     ctx->cases.resize(n_cases);
     for (int i = 0; i < n_cases; ++i) {
         Case& c = ctx->cases[i];
         c.d = desc[i];
         const nnlbm_case_desc& d = c.d;
         if (d.nx < 3 || d.ny < 3 || d.nz < 3 || d.dtype < 0 || d.dtype > 3 || d.collision < 0 || d.collision > 10 ||
-            d.equilibrium < 0 || d.equilibrium > 3 || d.cy_mode < 0 || d.cy_mode > 2 || !(d.nu > 0)) {
-            set_err(ctx, NNLBM_ERR_ARG, "case %d: invalid descriptor (dims >= 3, dtype 0..3, collision 0..10, "
-                    "equilibrium 0..3, cy_mode 0..2, nu > 0)", i);
-            *out = ctx;
-            return NNLBM_ERR_ARG;
-        }
-        if (d.cy_mode != NNLBM_CY_NONE && !(d.cy_a > 0 && d.cy_nu0 > 0)) {
-            set_err(ctx, NNLBM_ERR_ARG, "case %d: Carreau-Yasuda needs a > 0 and nu0 > 0", i);
-            *out = ctx;
-            return NNLBM_ERR_ARG;
-        }
+            d.equilibrium < 0 || d.equilibrium > 3 || d.cy_mode < 0 || d.cy_mode > 2 || !(d.nu > 0))
+            return set_err(ctx, NNLBM_ERR_ARG, "case %d: invalid descriptor (dims >= 3, dtype 0..3, collision 0..10, "
+                           "equilibrium 0..3, cy_mode 0..2, nu > 0)", i);
+        if (d.cy_mode != NNLBM_CY_NONE && !(d.cy_a > 0 && d.cy_nu0 > 0))
+            return set_err(ctx, NNLBM_ERR_ARG, "case %d: Carreau-Yasuda needs a > 0 and nu0 > 0", i);
+        if (d.ny > 65535 || d.nz > 65535) return set_err(ctx, NNLBM_ERR_ARG, "case %d: ny and nz are limited to 65535", i);
         c.N = (int64_t)d.nx * d.ny * d.nz;
-        if (c.N >= (int64_t)1 << 31) {
-            set_err(ctx, NNLBM_ERR_ARG, "case %d: %lld cells exceed 2^31", i, (long long)c.N);
-            *out = ctx;
-            return NNLBM_ERR_ARG;
-        }
+        if (c.N >= (int64_t)1 << 31) return set_err(ctx, NNLBM_ERR_ARG, "case %d: %lld cells exceed 2^31", i, (long long)c.N);
         c.ct_bytes = d.dtype == NNLBM_F64 ? 8 : 4;
-        c.scale = d.storage_scale > 0 ? d.storage_scale : (d.dtype == NNLBM_F16 ? 1024.0 : 1.0);
-        if (d.dtype == NNLBM_F64 || d.dtype == NNLBM_F32) c.scale = 1.0;
+        c.scale = (d.dtype == NNLBM_F16 || d.dtype == NNLBM_BF16) && d.storage_scale > 0 ? d.storage_scale
+                  : (d.dtype == NNLBM_F16 ? 1024.0 : 1.0);
         const size_t eb = kStorageBytes[d.dtype];
         c.q_stride = ((size_t)c.N + 127) / 128 * 128;
-        if (cudaMalloc(&c.df, 27 * c.q_stride * eb) != cudaSuccess ||
-            cudaMalloc(&c.d_label, (size_t)c.N) != cudaSuccess ||
-            cudaMalloc(&c.d_ints, 4 * sizeof(int)) != cudaSuccess || cudaMalloc(&c.d_red, 8 * sizeof(double)) != cudaSuccess) {
+        if (cudaMalloc(&c.df, 27 * c.q_stride * eb) != cudaSuccess || cudaMalloc(&c.d_label, (size_t)c.N) != cudaSuccess ||
+            cudaMalloc(&c.d_red, 8 * sizeof(double)) != cudaSuccess || cudaMalloc(&c.d_err, sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
-            set_err(ctx, NNLBM_ERR_OOM, "case %d: device allocation of %.2f GB failed", i, 27.0 * c.q_stride * eb / 1e9);
-            *out = ctx;
-            return NNLBM_ERR_OOM;
+            return set_err(ctx, NNLBM_ERR_OOM, "case %d: device allocation of %.2f GB failed", i, 27.0 * c.q_stride * eb / 1e9);
         }
-        cudaMemset(c.d_ints, 0, 4 * sizeof(int));
         cudaMemset(c.d_red, 0, 8 * sizeof(double));
-        c.label.assign((size_t)c.N, (uint8_t)NNLBM_WALL);
-        if (upload_ct(ctx, c, &c.d_bc_prof, {}) != NNLBM_OK || upload_ct(ctx, c, &c.d_bc_buf, {}) != NNLBM_OK) {
-            *out = ctx;
-            return NNLBM_ERR_OOM;
+        cudaMemset(c.d_err, 0, sizeof(int));
+        c.label.assign((size_t)c.N, (uint8_t)L_WALL);
+        c.dlabel = c.label;
+        // launch groups: cases of one storage type and collision run in the same kernels
+        int gi = -1;
+        for (size_t k = 0; k < ctx->groups.size(); ++k)
+            if (ctx->groups[k].dtype == d.dtype && ctx->groups[k].collision == d.collision) gi = (int)k;
+        if (gi < 0) {
+            ctx->groups.emplace_back();
+            gi = (int)ctx->groups.size() - 1;
+            ctx->groups[gi].dtype = d.dtype;
+            ctx->groups[gi].collision = d.collision;
+            if (cudaMalloc(&ctx->groups[gi].d_ints, 4 * sizeof(int)) != cudaSuccess)
+                return set_err(ctx, NNLBM_ERR_OOM, "device allocation failed");
+            cudaMemset(ctx->groups[gi].d_ints, 0, 4 * sizeof(int));
         }
+        c.group = gi;
+        ctx->groups[gi].cases.push_back(i);
         int rc = ensure_ctl(ctx, c, 1024);
-        if (rc != NNLBM_OK) { *out = ctx; return rc; }
-        rebuild_args(c);
+        if (rc != NNLBM_OK) return rc;
+        rebuild_case_args(ctx, c);
     }
-    (void)fail;
-    *out = ctx;
     return NNLBM_OK;
 }
 
@@ -433,13 +526,12 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
     if (!map) return set_err(ctx, NNLBM_ERR_ARG, "null map");
     Case& c = ctx->cases[ic];
     const int nx = c.d.nx, ny = c.d.ny, nz = c.d.nz;
-    int64_t nfl = 0, la = 0, ra = 0, neq = 0;
-    std::vector<int32_t> bcs;
+    auto id = [&](int x, int y, int z) { return (size_t)x + (size_t)nx * (y + (size_t)ny * z); };
+    int64_t nfl = 0, la = 0, ra = 0, neq = 0, nbc = 0;
     for (int z = 0; z < nz; ++z)
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) {
-                const int64_t i = x + (int64_t)nx * (y + (int64_t)ny * z);
-                const int lab = map[i];
+                const int lab = map[id(x, y, z)];
                 if (lab > L_OUT_REQ) return set_err(ctx, NNLBM_ERR_ARG, "label %d at (%d,%d,%d) is not a solver label", lab, x, y, z);
                 const bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
                 if (lab == L_FLUID && face)
@@ -454,40 +546,85 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 la += lab == L_IN_L;
                 ra += lab == L_IN_R;
                 neq += lab == L_IN_EQ;
-                if (is_bc(lab)) bcs.push_back((int32_t)i);
+                nbc += lab >= L_IN_L;
+            }
+    // work flags: which open-plane nodes are finished by the thread of their inward
+    // neighbour (same stencil, same force) and which need their own thread
+    std::vector<uint8_t> dl(map, map + c.N);
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const size_t i = id(x, y, z);
+                const int lab = map[i];
+                if (lab == L_IN_EQ) { dl[i] |= LF_SELF; continue; }
+                if (!is_pull_bc(lab)) continue;
+                const bool xnormal = lab == L_IN_L || lab == L_IN_R || lab == L_OUT_REQ;
+                const bool tangential_interior = xnormal ? (y > 0 && y < ny - 1 && z > 0 && z < nz - 1)
+                                                         : (x > 0 && x < nx - 1 && z > 0 && z < nz - 1);
+                int sx = x, sy = y;
+                if (lab == L_IN_L) sx = x + 1;
+                if (lab == L_IN_R || lab == L_OUT_REQ) sx = x - 1;
+                if (lab == L_OUT_F) sy = y + 1;
+                if (lab == L_OUT_B) sy = y - 1;
+                const int sl = map[id(sx, sy, z)];
+                const bool src_ok = sl == L_FLUID || sl == L_PERIODIC;
+                // under CY_REF_FD the source's velocity carries its own CY force
+                const bool force_ok = c.d.cy_mode != NNLBM_CY_REF_FD || lab == L_IN_L || lab == L_IN_R;
+                if (tangential_interior && src_ok && force_ok) {
+                    dl[i] |= LF_FUSED;
+                    dl[id(sx, sy, z)] |= LF_SOURCE;
+                } else {
+                    dl[i] |= LF_SELF;
+                }
+            }
+    // packed work list of 32-cell row chunks and the self-handled nodes
+    std::vector<int4> chunks;
+    std::vector<int32_t> self_cell, gather_self;
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x0 = 0; x0 < nx; x0 += kChunk) {
+                const int self_base = (int)self_cell.size();
+                bool work = false;
+                for (int x = x0; x < std::min(nx, x0 + kChunk); ++x) {
+                    const size_t i = id(x, y, z);
+                    const int lab = map[i];
+                    if (lab == L_FLUID || lab == L_PERIODIC) work = true;
+                    if (dl[i] & LF_SELF) {
+                        work = true;
+                        if (lab != L_IN_EQ) gather_self.push_back((int32_t)self_cell.size());
+                        self_cell.push_back((int32_t)i);
+                    }
+                }
+                if (work) chunks.push_back(make_int4((int)id(x0, y, z), y | (z << 16), 0, self_base));
             }
     c.label.assign(map, map + c.N);
-    c.bc_cell = bcs;
-    c.bc_prof.assign(bcs.size() * 3, 0.0);
-    c.n_fluid = nfl; c.left_area = la; c.right_area = ra; c.n_inflow_eq = neq;
+    c.dlabel = dl;
+    c.chunks = chunks;
+    c.self_cell = self_cell;
+    c.gather_self = gather_self;
+    c.self_prof.assign(self_cell.size() * 3, 0.0);
+    c.n_fluid = nfl; c.left_area = la; c.right_area = ra; c.n_inflow_eq = neq; c.n_bc = nbc;
     CK(cudaSetDevice(ctx->device));
-    CK(cudaMemcpy(c.d_label, map, (size_t)c.N, cudaMemcpyHostToDevice));
-    if (c.d_bc_cell) { cudaFree(c.d_bc_cell); c.d_bc_cell = nullptr; }
-    CK(cudaMalloc(&c.d_bc_cell, std::max<size_t>(bcs.size(), 1) * sizeof(int32_t)));
-    if (!bcs.empty()) CK(cudaMemcpy(c.d_bc_cell, bcs.data(), bcs.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    if ((rc = upload_ct(ctx, c, &c.d_bc_prof, c.bc_prof)) != NNLBM_OK) return rc;
-    std::vector<double> zeros(bcs.size() * 4, 0.0);
-    if ((rc = upload_ct(ctx, c, &c.d_bc_buf, zeros)) != NNLBM_OK) return rc;
+    CK(cudaMemcpy(c.d_label, dl.data(), (size_t)c.N, cudaMemcpyHostToDevice));
     c.has_map = true;
-    rebuild_args(c);
+    rebuild_case_args(ctx, c);
     return NNLBM_OK;
 }
 
 // StateTcpc::setupBoundaries (sim_tcpc.cu:494-645) + LBM::projectWall (lbm.hpp:144-155)
-int nnlbm_setup_tcpc(nnlbm_ctx* ctx, int ic, const int32_t* wall, int64_t* counts)
+int nnlbm_tcpc_labels(int32_t X, int32_t Y, int32_t Z, const int32_t* wall, uint8_t* map_out, int64_t* counts)
 {
-    int rc = check_case(ctx, ic);
-    if (rc) return rc;
-    if (!wall) return set_err(ctx, NNLBM_ERR_ARG, "null wall array");
-    Case& c = ctx->cases[ic];
-    const int X = c.d.nx, Y = c.d.ny, Z = c.d.nz;
+    if (X < 3 || Y < 3 || Z < 3 || !wall || !map_out) return NNLBM_ERR_ARG;
+    const size_t N = (size_t)X * Y * Z;
     auto id = [&](int x, int y, int z) { return (size_t)x + (size_t)X * (y + (size_t)Y * z); };
-    std::vector<uint8_t> map((size_t)c.N, (uint8_t)L_FLUID), wf((size_t)c.N, 0);
+    uint8_t* map = map_out;
+    std::vector<uint8_t> wf(N, 0);
     int64_t in[7] = {0};
-    for (size_t i = 0; i < (size_t)c.N; ++i) {
+    for (size_t i = 0; i < N; ++i) {
         const int lab = wall[i];
         if (lab >= 3 && lab <= 6) in[lab]++;
         wf[i] = lab == 1;
+        map[i] = L_FLUID;
     }
     // plane labels; later calls win at edges (sim_tcpc.cu:524-529)
     for (int z = 0; z < Z; ++z)
@@ -500,9 +637,9 @@ int nnlbm_setup_tcpc(nnlbm_ctx* ctx, int ic, const int32_t* wall, int64_t* count
     // (openBoundaryX / openBoundaryY, sim_tcpc.cu:531-586)
     auto open_plane = [&](int axis, int b, int step) {
         const int n = axis == 0 ? X : Y;
-        int s = b + step;
-        auto cell = [&](int a, int u, int z) { return axis == 0 ? id(a, u, z) : id(u, a, z); };
         const int nu = axis == 0 ? Y : X;
+        auto cell = [&](int a, int u, int z) { return axis == 0 ? id(a, u, z) : id(u, a, z); };
+        int s = b + step;
         while (s > 0 && s < n - 1) {
             int64_t open = 0;
             for (int z = 0; z < Z; ++z)
@@ -521,24 +658,37 @@ int nnlbm_setup_tcpc(nnlbm_ctx* ctx, int ic, const int32_t* wall, int64_t* count
     open_plane(1, 0, 1);
     open_plane(1, Y - 1, -1);
     int64_t la = 0, ra = 0, of = 0, ob = 0, wc = 0, fc = 0;
-    for (size_t i = 0; i < (size_t)c.N; ++i) {
+    for (size_t i = 0; i < N; ++i) {
         const int lab = map[i];
         const bool w = wf[i] || lab == L_WALL;
         la += lab == L_IN_L && !w; ra += lab == L_IN_R && !w;
         of += lab == L_OUT_F && !w; ob += lab == L_OUT_B && !w;
         wc += w; fc += lab == L_FLUID && !w;
     }
-    for (size_t i = 0; i < (size_t)c.N; ++i)
+    for (size_t i = 0; i < N; ++i)
         if (wf[i]) map[i] = L_WALL;
     if (counts) {
         const int64_t v[10] = {la, ra, of, ob, wc, fc, in[3], in[4], in[5], in[6]};
         memcpy(counts, v, sizeof v);
     }
+    return (la <= 0 || ra <= 0 || of <= 0 || ob <= 0) ? NNLBM_ERR_AREA : NNLBM_OK;
+}
+
+int nnlbm_setup_tcpc(nnlbm_ctx* ctx, int ic, const int32_t* wall, int64_t* counts)
+{
+    int rc = check_case(ctx, ic);
+    if (rc) return rc;
+    if (!wall) return set_err(ctx, NNLBM_ERR_ARG, "null wall array");
+    Case& c = ctx->cases[ic];
+    std::vector<uint8_t> map((size_t)c.N);
+    int64_t cnt[10];
+    const int lrc = nnlbm_tcpc_labels(c.d.nx, c.d.ny, c.d.nz, wall, map.data(), cnt);
+    if (counts) memcpy(counts, cnt, sizeof cnt);
     if ((rc = nnlbm_set_map(ctx, ic, map.data())) != NNLBM_OK) return rc;
-    if (la <= 0 || ra <= 0 || of <= 0 || ob <= 0)
+    if (lrc == NNLBM_ERR_AREA)
         return set_err(ctx, NNLBM_ERR_AREA, "zero inlet or outlet area: left=%lld right=%lld outlet5=%lld outlet6=%lld",
-                       (long long)la, (long long)ra, (long long)of, (long long)ob);
-    return NNLBM_OK;
+                       (long long)cnt[0], (long long)cnt[1], (long long)cnt[2], (long long)cnt[3]);
+    return lrc;
 }
 
 int nnlbm_init_equilibrium(nnlbm_ctx* ctx, int ic, double rho, double ux, double uy, double uz)
@@ -548,12 +698,12 @@ int nnlbm_init_equilibrium(nnlbm_ctx* ctx, int ic, double rho, double ux, double
     Case& c = ctx->cases[ic];
     if (!c.has_map) return set_err(ctx, NNLBM_ERR_ARG, "set the map before the initial state");
     CK(cudaSetDevice(ctx->device));
-    const BcLaunchers& B = bc_launchers(c.d.dtype);
-    B.fill_eq(c.args.data(), rho, ux, uy, uz, ctx->stream);
+    const AuxLaunchers& A = aux_launchers(c.d.dtype);
+    A.fill_eq(c.args.data(), rho, ux, uy, uz, ctx->stream);
     CK(cudaGetLastError());
-    if (c.d_macro) B.init_macro(c.args.data(), rho, ux, uy, uz, ctx->stream);
+    if (c.d_macro) A.init_macro(c.args.data(), rho, ux, uy, uz, ctx->stream);
     if (c.d_stats) CK(cudaMemsetAsync(c.d_stats, 0, (size_t)6 * c.N * (c.d.stats_f64 ? 8 : 4), ctx->stream));
-    CK(cudaMemsetAsync(c.d_ints, 0, 3 * sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(c.d_err, 0, sizeof(int), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     c.parity = 0; c.iterations = 0; c.n_stats = 0;
     c.has_state = true;
@@ -578,14 +728,12 @@ int nnlbm_set_inflow_profile(nnlbm_ctx* ctx, int ic, const double* u, int64_t n)
         return set_err(ctx, NNLBM_ERR_ARG, "profile has %lld rows, the map has %lld INFLOW_EQ cells", (long long)n,
                        (long long)c.n_inflow_eq);
     int64_t k = 0;
-    for (size_t b = 0; b < c.bc_cell.size(); ++b)
-        if (c.label[c.bc_cell[b]] == L_IN_EQ) {
-            for (int j = 0; j < 3; ++j) c.bc_prof[3 * b + j] = u[3 * k + j];
+    for (size_t s = 0; s < c.self_cell.size(); ++s)
+        if (c.label[c.self_cell[s]] == L_IN_EQ) {
+            for (int j = 0; j < 3; ++j) c.self_prof[3 * s + j] = u[3 * k + j];
             ++k;
         }
-    CK(cudaSetDevice(ctx->device));
-    if ((rc = upload_ct(ctx, c, &c.d_bc_prof, c.bc_prof)) != NNLBM_OK) return rc;
-    rebuild_args(c);
+    ctx->groups[c.group].dirty = true;
     return NNLBM_OK;
 }
 
@@ -604,29 +752,18 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
     if (n_steps < 0) return set_err(ctx, NNLBM_ERR_ARG, "negative step count");
     if (n_steps == 0) return NNLBM_OK;
     CK(cudaSetDevice(ctx->device));
-    for (size_t i = 0; i < ctx->cases.size(); ++i) {
-        Case& c = ctx->cases[i];
-        if (!c.has_map || !c.has_state) return set_err(ctx, NNLBM_ERR_ARG, "case %zu has no map or initial state", i);
-        int rc = run_case_steps(ctx, c, n_steps, flags, true);
+    for (Group& g : ctx->groups) {
+        int rc = run_group_steps(ctx, g, n_steps, flags, true);
         if (rc != NNLBM_OK) return rc;
-        if (!c.sched.empty()) {
-            // consume the rows that were used
-            const int64_t used = std::min<int64_t>(n_steps, (int64_t)c.sched.size() / 3);
-            if (used < (int64_t)c.sched.size() / 3) c.sched.erase(c.sched.begin(), c.sched.begin() + 3 * used);
-            else c.sched.erase(c.sched.begin(), c.sched.end() - 3); // keep the last row
-        }
     }
-    std::vector<int> errs(ctx->cases.size() * 3);
-    for (size_t i = 0; i < ctx->cases.size(); ++i)
-        CK(cudaMemcpyAsync(&errs[3 * i], ctx->cases[i].d_ints, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    for (size_t i = 0; i < ctx->cases.size(); ++i) {
-        if (errs[3 * i] != n_steps)
-            return set_err(ctx, NNLBM_ERR_CUDA, "case %zu: step cursor %d after %lld steps", i, errs[3 * i], (long long)n_steps);
-        if (errs[3 * i + 2])
-            return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
+    for (Case& c : ctx->cases) {
+        if (c.sched.empty()) continue;
+        // consume the rows that were used; the last row stays in force
+        const int64_t rows = (int64_t)c.sched.size() / 3;
+        if (n_steps < rows) c.sched.erase(c.sched.begin(), c.sched.begin() + 3 * n_steps);
+        else c.sched.erase(c.sched.begin(), c.sched.end() - 3);
     }
-    return NNLBM_OK;
+    return wait_and_check(ctx, n_steps);
 }
 
 int nnlbm_stat_reset(nnlbm_ctx* ctx, int ic)
@@ -744,50 +881,62 @@ int nnlbm_autotune(nnlbm_ctx* ctx)
 {
     if (!ctx) return NNLBM_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
-    static const int shapes[][2] = {{32, 4}, {32, 8}, {64, 2}, {64, 4}, {128, 1}, {128, 2}, {256, 1}};
-    for (Case& c : ctx->cases) {
-        if (!c.has_map || !c.has_state) continue;
-        // tune on a copy of the state so that the lattice does not advance
-        const size_t eb = kStorageBytes[c.d.dtype];
-        const size_t bytes = 27 * c.q_stride * eb;
-        void* save = nullptr;
-        CK(cudaMalloc(&save, bytes));
-        CK(cudaMemcpyAsync(save, c.df, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-        void* msave = nullptr;
-        const size_t mbytes = (size_t)M_N * c.N * c.ct_bytes;
-        if (c.d_macro) {
-            CK(cudaMalloc(&msave, mbytes));
-            CK(cudaMemcpyAsync(msave, c.d_macro, mbytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    static const int blocks[] = {64, 128, 256};
+    for (Group& g : ctx->groups) {
+        bool ready = true;
+        for (int ic : g.cases) ready = ready && ctx->cases[ic].has_map && ctx->cases[ic].has_state;
+        if (!ready) continue;
+        // tune on copies of the states so that the lattices do not advance
+        std::vector<void*> saved, msaved;
+        for (int ic : g.cases) {
+            Case& c = ctx->cases[ic];
+            const size_t bytes = 27 * c.q_stride * kStorageBytes[c.d.dtype];
+            void* p = nullptr;
+            CK(cudaMalloc(&p, bytes));
+            CK(cudaMemcpyAsync(p, c.df, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+            saved.push_back(p);
+            void* m = nullptr;
+            if (c.d_macro) {
+                const size_t mb = (size_t)M_N * c.N * c.ct_bytes;
+                CK(cudaMalloc(&m, mb));
+                CK(cudaMemcpyAsync(m, c.d_macro, mb, cudaMemcpyDeviceToDevice, ctx->stream));
+            }
+            msaved.push_back(m);
         }
-        const int64_t parity0 = c.parity, it0 = c.iterations;
+        std::vector<int64_t> par, it;
+        for (int ic : g.cases) { par.push_back(ctx->cases[ic].parity); it.push_back(ctx->cases[ic].iterations); }
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         float best = 1e30f;
-        int bbx = c.bx, bby = c.by;
-        for (auto& s : shapes) {
-            c.bx = s[0]; c.by = s[1];
-            int rc = run_case_steps(ctx, c, 2, 0, false);
+        int bb = g.block;
+        for (int b : blocks) {
+            g.block = b;
+            int rc = run_group_steps(ctx, g, 2, 0, false);
             if (rc) return rc;
             CK(cudaEventRecord(e0, ctx->stream));
-            rc = run_case_steps(ctx, c, 6, 0, false);
+            rc = run_group_steps(ctx, g, 6, 0, false);
             if (rc) return rc;
             CK(cudaEventRecord(e1, ctx->stream));
             CK(cudaEventSynchronize(e1));
             float ms = 0;
             CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) { best = ms; bbx = s[0]; bby = s[1]; }
+            if (ms < best) { best = ms; bb = b; }
         }
-        c.bx = bbx; c.by = bby;
-        c.parity = parity0; c.iterations = it0;
-        CK(cudaMemcpyAsync(c.df, save, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-        if (msave) CK(cudaMemcpyAsync(c.d_macro, msave, mbytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        g.block = bb;
+        g.gen++; // the graphs captured another launch shape
+        for (size_t j = 0; j < g.cases.size(); ++j) {
+            Case& c = ctx->cases[g.cases[j]];
+            c.parity = par[j]; c.iterations = it[j];
+            CK(cudaMemcpyAsync(c.df, saved[j], 27 * c.q_stride * kStorageBytes[c.d.dtype], cudaMemcpyDeviceToDevice, ctx->stream));
+            if (msaved[j]) CK(cudaMemcpyAsync(c.d_macro, msaved[j], (size_t)M_N * c.N * c.ct_bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
         CK(cudaStreamSynchronize(ctx->stream));
-        cudaFree(save);
-        if (msave) cudaFree(msave);
+        for (void* p : saved) cudaFree(p);
+        for (void* p : msaved)
+            if (p) cudaFree(p);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        c.gen++; // the graph captured the old launch shape
     }
     return NNLBM_OK;
 }
@@ -798,9 +947,12 @@ int nnlbm_step_info(nnlbm_ctx* ctx, int ic, int64_t* fluid_cells, int64_t* bc_ce
     int rc = check_case(ctx, ic);
     if (rc) return rc;
     Case& c = ctx->cases[ic];
+    Group& g = ctx->groups[c.group];
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = prepare_group(ctx, g)) != NNLBM_OK) return rc;
     if (fluid_cells) *fluid_cells = c.n_fluid;
-    if (bc_cells) *bc_cells = (int64_t)c.bc_cell.size();
-    if (launches_per_step) *launches_per_step = c.d.cy_mode == NNLBM_CY_REF_FD ? 5 : 3;
+    if (bc_cells) *bc_cells = c.n_bc;
+    if (launches_per_step) *launches_per_step = 1 + (g.n_gather > 0 ? 1 : 0) + (g.any_refd ? 2 : 0);
     if (bytes_per_step) *bytes_per_step = (double)c.n_fluid * (54.0 * kStorageBytes[c.d.dtype] + 1.0);
     return NNLBM_OK;
 }
@@ -810,65 +962,51 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
     int rc = check_case(ctx, ic);
     if (rc) return rc;
     if (!ms || !launches || n_steps < 1) return set_err(ctx, NNLBM_ERR_ARG, "bad profile arguments");
-    Case& c = ctx->cases[ic];
-    if (!c.has_map || !c.has_state) return set_err(ctx, NNLBM_ERR_ARG, "case has no map or initial state");
     CK(cudaSetDevice(ctx->device));
-    if ((flags & NNLBM_STEP_MACRO) || c.d.cy_mode == NNLBM_CY_REF_FD)
-        if ((rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
-    if (flags & NNLBM_STEP_STATS)
-        if ((rc = ensure_stats(ctx, c)) != NNLBM_OK) return rc;
-    if ((rc = ensure_ctl(ctx, c, n_steps)) != NNLBM_OK) return rc;
-    std::vector<char> buf;
-    if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n_steps, flags);
-    else fill_ctl<float>(c, buf, n_steps, flags);
-    CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemsetAsync(c.d_ints, 0, 2 * sizeof(int), ctx->stream));
-    const BcLaunchers& B = bc_launchers(c.d.dtype);
-    const dim3 blk(c.bx, c.by, 1);
-    const dim3 grd((c.d.nx + c.bx - 1) / c.bx, (c.d.ny + c.by - 1) / c.by, c.d.nz);
-    const int nbc = (int)c.bc_cell.size();
-    const dim3 bgrd((std::max(nbc, 1) + 127) / 128), bblk(128);
-    const bool refd = c.d.cy_mode == NNLBM_CY_REF_FD;
-    const int nk = refd ? 5 : 3;
-    std::vector<cudaEvent_t> ev((size_t)n_steps * (nk + 1));
-    for (auto& e : ev) CK(cudaEventCreate(&e));
+    Group& g = ctx->groups[ctx->cases[ic].group];
+    if ((rc = prepare_steps(ctx, g, n_steps, flags)) != NNLBM_OK) return rc;
+    const AuxLaunchers& A = aux_launchers(g.dtype);
+    const int per_block = g.block / kChunk;
+    const dim3 cgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block), cblk(g.block);
+    for (int i = 0; i < 5; ++i) { ms[i] = 0; launches[i] = 0; }
+    const int64_t parity = ctx->cases[g.cases[0]].parity;
+    // kinds: 0 gather, 1 step, 3 CY_REF_FD velocity, 4 CY_REF_FD strain
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;
+    auto mark = [&](int k) -> int {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return -1;
+        ev.push_back(e);
+        kind.push_back(k);
+        return cudaEventRecord(e, ctx->stream) == cudaSuccess ? 0 : -1;
+    };
     for (int64_t k = 0; k < n_steps; ++k) {
-        const bool odd = ((c.parity + k) & 1) != 0;
-        cudaEvent_t* e = &ev[(size_t)k * (nk + 1)];
-        int j = 0;
-        CK(cudaEventRecord(e[j++], ctx->stream));
-        if (refd) {
-            B.refd_velocity(odd, grd, blk, ctx->stream, c.args.data());
-            CK(cudaEventRecord(e[j++], ctx->stream));
-            B.refd_stress(odd, grd, blk, ctx->stream, c.args.data());
-            CK(cudaEventRecord(e[j++], ctx->stream));
+        const bool odd = ((parity + k) & 1) != 0;
+        if (mark(-1)) return set_err(ctx, NNLBM_ERR_CUDA, "event record failed");
+        if (g.any_refd) {
+            A.refd_velocity(odd, cgrid, cblk, ctx->stream, g.args.data());
+            mark(3);
+            A.refd_stress(odd, cgrid, cblk, ctx->stream, g.args.data());
+            mark(4);
         }
-        B.gather(odd, bgrd, bblk, ctx->stream, c.args.data());
-        CK(cudaEventRecord(e[j++], ctx->stream));
-        step_launcher(c.d.dtype, c.d.collision)(odd, grd, blk, ctx->stream, c.args.data());
-        CK(cudaEventRecord(e[j++], ctx->stream));
-        B.write(odd, bgrd, bblk, ctx->stream, c.args.data());
-        CK(cudaEventRecord(e[j++], ctx->stream));
+        if (g.n_gather > 0) {
+            A.gather(odd, dim3((g.n_gather + 127) / 128), dim3(128), ctx->stream, g.args.data());
+            mark(0);
+        }
+        step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, g.args.data());
+        mark(1);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(ctx->stream));
-    for (int i = 0; i < 5; ++i) { ms[i] = 0; launches[i] = 0; }
-    // kinds in launch order: [refd velocity, refd strain,] gather, step, write
-    const int kinds_refd[5] = {3, 4, 0, 1, 2}, kinds[3] = {0, 1, 2};
-    for (int64_t k = 0; k < n_steps; ++k) {
-        cudaEvent_t* e = &ev[(size_t)k * (nk + 1)];
-        for (int j = 0; j < nk; ++j) {
-            float t = 0;
-            CK(cudaEventElapsedTime(&t, e[j], e[j + 1]));
-            const int kind = refd ? kinds_refd[j] : kinds[j];
-            ms[kind] += t;
-            launches[kind] += 1;
-        }
+    for (size_t i = 1; i < ev.size(); ++i) {
+        if (kind[i] < 0) continue;
+        float t = 0;
+        CK(cudaEventElapsedTime(&t, ev[i - 1], ev[i]));
+        ms[kind[i]] += t;
+        launches[kind[i]] += 1;
     }
     for (auto& e : ev) cudaEventDestroy(e);
-    c.parity = (c.parity + n_steps) & 1;
-    c.iterations += n_steps;
-    if (flags & NNLBM_STEP_STATS) c.n_stats += n_steps;
+    finish_steps(ctx, g, n_steps, flags);
     return NNLBM_OK;
 }
 
@@ -889,10 +1027,15 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
     if (!ctx) return NNLBM_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (Case& c : ctx->cases) {
+    for (Group& g : ctx->groups) {
         for (int p = 0; p < 2; ++p)
-            if (c.graph[p]) cudaGraphExecDestroy(c.graph[p]);
-        void* ptrs[] = {c.df, c.d_label, c.d_bc_cell, c.d_bc_prof, c.d_bc_buf, c.d_macro, c.d_stats, c.d_ctl, c.d_ints, c.d_red};
+            if (g.graph[p]) cudaGraphExecDestroy(g.graph[p]);
+        void* ptrs[] = {g.d_cases, g.d_chunks, g.d_gather, g.d_bc_prof, g.d_bc_buf, g.d_ints};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+    }
+    for (Case& c : ctx->cases) {
+        void* ptrs[] = {c.df, c.d_label, c.d_macro, c.d_stats, c.d_ctl, c.d_red, c.d_err};
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }

@@ -14,12 +14,18 @@
 // solver/sim_tcpc/sim_tcpc.cu:235-241) need no work at all under A-A: their post-step
 // value f*_q = incoming f_opp(q) already sits in the slot the neighbour reads next.
 //
-// The open-plane nodes (TCPC inflow/outflow, generic GEO_INFLOW / GEO_OUTFLOW_RIGHT_EQ) pull
-// a re-centred stencil from a neighbour (sim_tcpc.cu:242-273, lbm_bc.h:126-152).  Those
-// reads touch slots that the neighbour overwrites in the same step, so one step is three
-// launches: k_bc_gather (the re-centred moments of every boundary node, before anything is
-// written), k_step (FLUID and PERIODIC cells), k_bc_write (equilibria of the boundary
-// nodes into their own slots).
+// Work decomposition: a packed list of 32-cell row chunks (one warp each) that contain a
+// cell with work, over all cases of a launch group (same storage type and collision).
+// Per-case parameters live in a device array indexed by the chunk's case.
+//
+// Open-plane nodes (TCPC IVC/SVC inflow and outlets, generic GEO_OUTFLOW_RIGHT_EQ) pull a
+// stencil re-centred one cell inward (sim_tcpc.cu:242-273, lbm_bc.h:147-152).  Those
+// populations are exactly the ones the inward neighbour pulls for itself, so when that
+// neighbour is a FLUID/PERIODIC cell with the same tangential stencil ("source") its own
+// thread computes the node's density / velocity and writes the node's equilibrium into
+// the node's slots (which no other cell touches within the step).  The remaining nodes
+// (corners, CY_REF_FD outlets) are gathered by k_bc_gather before the step kernel and
+// written by their own thread; GEO_INFLOW nodes need no gather at all.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -33,6 +39,8 @@ namespace nnlbm {
 
 enum : int { L_FLUID = 0, L_WALL = 1, L_PERIODIC = 2, L_IN_L = 3, L_IN_R = 4, L_OUT_F = 5, L_OUT_B = 6,
              L_IN_EQ = 7, L_OUT_REQ = 8 };
+// flag bits of the device label byte (the low four bits hold the label)
+enum : int { LF_SOURCE = 0x80, LF_SELF = 0x40, LF_FUSED = 0x20, L_MASK = 0x0f };
 enum : int { CY_NONE = 0, CY_REF_FD = 1, CY_LOCAL_NEQ = 2 };
 enum : int { F_STATS = 1, F_MACRO = 2, F_REDUCE = 4 };
 // macro field order of the context's macro array
@@ -64,8 +72,8 @@ template <> struct Storage<3> {
     __device__ static __forceinline__ void store(T* p, int i, int q, CT v, CT sc) { p[i] = __float2bfloat16_rn((v - weight<float>(q)) * sc); }
 };
 
-// per-step control word written by the host before each nnlbm_step call and indexed by a
-// device cursor that k_bc_write advances, so a captured graph replays any schedule
+// per-step control row written by the host before each nnlbm_step call and indexed by a
+// device cursor that the step kernel advances, so one captured graph replays any schedule
 template <class CT>
 struct StepCtl {
     int flags;
@@ -74,10 +82,12 @@ struct StepCtl {
     CT rho_left, rho_right, rho_eq, prof_scale;
 };
 
+// everything a kernel needs to know about one case
 template <class CT>
-struct KArgs {
-    void* dfq[27];             // per-direction base pointers
-    const uint8_t* label;      // [N]
+struct CaseArgs {
+    void* df;                  // 27 direction arrays, qstride elements apart
+    int64_t qstride;
+    const uint8_t* label;      // [N] label | flag bits
     int nx, ny, nz, pad0;
     int64_t N;
     CT nu, nu0, lam, a, n;     // viscosity (nu_inf for CY) and Carreau-Yasuda parameters
@@ -88,46 +98,162 @@ struct KArgs {
     void* stats;               // [6][N] (double or float) or null
     int stats_f64, pad1;
     const StepCtl<CT>* ctl;
-    int* cursor;
-    int* done;                 // block counter of k_bc_write
     double* red;               // [5] mass, Q_ivc, Q_svc, Q_out5, Q_out6
     int* err;                  // watchdog flag
-    const int32_t* bc_cell;    // [n_bc] cell index of every open-plane node
-    const CT* bc_prof;         // [n_bc][3] prescribed velocity (INFLOW_EQ nodes)
-    CT* bc_buf;                // [n_bc][4] rho, ux, uy, uz of the current step
-    int n_bc, pad2;
 };
+
+// a launch group: cases sharing storage type and collision
+template <class CT>
+struct GroupArgs {
+    const CaseArgs<CT>* cases;
+    const int4* chunks;        // {first cell, y | z << 16, case, first self-node index}
+    int n_chunks, pad0;
+    const int4* gather;        // {cell, case, self-node index, 0} of the gathered nodes
+    int n_gather, pad1;
+    const CT* bc_prof;         // [n_self][3] prescribed velocity (GEO_INFLOW nodes)
+    CT* bc_buf;                // [n_self][4] gathered rho, ux, uy, uz
+    int* cursor;               // step cursor into every case's ctl
+    int* done;                 // block counter of the step kernel
+};
+
+template <int DT>
+__device__ __forceinline__ typename Storage<DT>::T* qptr(const CaseArgs<typename Storage<DT>::CT>& a, int q)
+{
+    return (typename Storage<DT>::T*)a.df + (int64_t)q * a.qstride;
+}
 
 __device__ __forceinline__ int wrapc(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
-template <class CT>
-__device__ __forceinline__ void warp_add_double(double v, double* dst)
+__device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x + blockDim.x * threadIdx.y) % 32 == 0 && v != 0.0) atomicAdd(dst, v);
+    return v;
 }
 
 template <class CT>
-__device__ __forceinline__ void accumulate_stats(const KArgs<CT>& a, int64_t c, CT rho, CT ux, CT uy, CT uz)
+__device__ __forceinline__ void accumulate_stats(const CaseArgs<CT>& a, int c, CT rho, CT ux, CT uy, CT uz)
 {
     // MacroTcpc::outputMacro (sim_tcpc.cu:347-353); the sign split of rho*ux is summed
     const CT jx = rho * ux, jy = rho * uy, jz = rho * uz;
+    const int64_t N = a.N;
     if (a.stats_f64) {
         double* s = (double*)a.stats;
-        s[c] += (double)jx; s[a.N + c] += (double)jy; s[2 * a.N + c] += (double)jz;
-        s[3 * a.N + c] += (double)jx * (double)jx; s[4 * a.N + c] += (double)jy * (double)jy;
-        s[5 * a.N + c] += (double)jz * (double)jz;
+        s[c] += (double)jx; s[N + c] += (double)jy; s[2 * N + c] += (double)jz;
+        s[3 * N + c] += (double)jx * (double)jx; s[4 * N + c] += (double)jy * (double)jy;
+        s[5 * N + c] += (double)jz * (double)jz;
     } else {
         float* s = (float*)a.stats;
-        s[c] += (float)jx; s[a.N + c] += (float)jy; s[2 * a.N + c] += (float)jz;
-        s[3 * a.N + c] += (float)(jx * jx); s[4 * a.N + c] += (float)(jy * jy); s[5 * a.N + c] += (float)(jz * jz);
+        s[c] += (float)jx; s[N + c] += (float)jy; s[2 * N + c] += (float)jz;
+        s[3 * N + c] += (float)(jx * jx); s[4 * N + c] += (float)(jy * jy); s[5 * N + c] += (float)(jz * jz);
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// the fused step for FLUID and PERIODIC cells (solver/lbm3d/core.h:578-800)
-// ---------------------------------------------------------------------------------------
+template <class CT>
+__device__ __forceinline__ void write_macro(const CaseArgs<CT>& a, int c, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz)
+{
+    CT* M = a.macro;
+    const int64_t N = a.N;
+    M[M_RHO * N + c] = rho; M[M_VX * N + c] = ux; M[M_VY * N + c] = uy; M[M_VZ * N + c] = uz;
+    M[M_FX * N + c] = fx; M[M_FY * N + c] = fy; M[M_FZ * N + c] = fz;
+}
+
+// Carreau-Yasuda viscosity of the reference's finite-difference coupling (core.h:763-766),
+// evaluated in single precision as the reference's powf does; in FP64 builds the power is
+// taken in double and rounded once so that the value is the correctly rounded float
+template <class CT>
+__device__ __forceinline__ CT ref_cy_nu(CT nu, CT nu0, CT gam, CT lam, CT a, CT n);
+template <>
+__device__ __forceinline__ float ref_cy_nu<float>(float nu, float nu0, float gam, float lam, float a, float n)
+{
+    return nu + (nu0 - nu) * powf(1.0f + powf(gam * lam, a), (n - 1.0f) / a);
+}
+template <>
+__device__ __forceinline__ double ref_cy_nu<double>(double nu, double nu0, double gam, double lam, double a, double n)
+{
+    const float inner = (float)pow((double)(float)(gam * lam), (double)(float)a);
+    const float outer = (float)pow((double)(float)(1.0 + (double)inner), (double)(float)((n - 1.0) / a));
+    return nu + (nu0 - nu) * (double)outer;
+}
+
+// write the equilibrium of an open-plane node into its own slots (A-A layout of this step)
+template <int DT, bool ODD>
+__device__ __forceinline__ void store_node_eq(const CaseArgs<typename Storage<DT>::CT>& a, int c, int x, int y, int z,
+                                              typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
+                                              typename Storage<DT>::CT uy, typename Storage<DT>::CT uz)
+{
+    using S = Storage<DT>;
+    using CT = typename S::CT;
+    CT f[27];
+    equilibrium<CT>(a.eq, rho, ux, uy, uz, f);
+    const int sy = a.nx, sz = a.nx * a.ny;
+    if (!ODD) {
+#pragma unroll
+        for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, oppq(q)), c, q, f[q], a.scale);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 27; ++q)
+            S::store(qptr<DT>(a, q), wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz), q, f[q],
+                     a.scale);
+    }
+}
+
+// macro / stats / flux bookkeeping of an open-plane node
+template <class CT>
+__device__ __forceinline__ void node_outputs(const CaseArgs<CT>& a, int flags, int lab, int c, CT rho, CT ux, CT uy, CT uz,
+                                             double* qf)
+{
+    if ((flags & F_MACRO) || a.cy_mode == CY_REF_FD) write_macro<CT>(a, c, rho, ux, uy, uz, a.fx, a.fy, a.fz);
+    if (flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
+    // plane fluxes of postprocess/compute_flows.py:107-147, inflow positive at 3/4
+    if (lab == L_IN_L) qf[0] += (double)ux;
+    if (lab == L_IN_R) qf[1] -= (double)ux;
+    if (lab == L_OUT_F) qf[2] -= (double)uy;
+    if (lab == L_OUT_B) qf[3] += (double)uy;
+}
+
+// rare paths of the step kernel are kept out of line so that they do not take registers
+// from the bulk path: the equilibrium of an open-plane node with its bookkeeping ...
+template <int DT, bool ODD>
+__device__ __noinline__ void finish_node(const CaseArgs<typename Storage<DT>::CT>& a, int flags, int lab, int c, int x, int y, int z,
+                                         typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
+                                         typename Storage<DT>::CT uy, typename Storage<DT>::CT uz, double* qf)
+{
+    store_node_eq<DT, ODD>(a, c, x, y, z, rho, ux, uy, uz);
+    node_outputs<typename Storage<DT>::CT>(a, flags, lab, c, rho, ux, uy, uz, qf);
+}
+
+// ... and the finite-difference Carreau-Yasuda force of CY_REF_FD (core.h:663-781):
+// divergence of the strain of the previous phase with one-sided differences next to
+// non-FLUID cells, then 2 (nu(gamma) - nu) F rho with rho still at its default of 1
+template <class CT>
+__device__ __noinline__ void refd_force(const CaseArgs<CT>& a, int c, int sy, int sz, CT* F)
+{
+    const CT* M = a.macro;
+    const int64_t N = a.N;
+    const int cn[6] = {c - 1, c + 1, c - sy, c + sy, c - sz, c + sz};
+    bool fl[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) fl[k] = (a.label[cn[k]] & L_MASK) == L_FLUID;
+    auto d1 = [&](int fld, int axis) -> CT {
+        const bool m = fl[2 * axis], p = fl[2 * axis + 1];
+        const CT* Fd = M + (int64_t)fld * N;
+        if (!m) return p ? Fd[cn[2 * axis + 1]] - Fd[c] : CT(0);
+        if (!p) return Fd[c] - Fd[cn[2 * axis]];
+        return CT(0.5) * (Fd[cn[2 * axis + 1]] - Fd[cn[2 * axis]]);
+    };
+    const CT F1 = d1(M_S11, 0) + d1(M_S12, 1) + d1(M_S13, 2);
+    const CT F2 = d1(M_S12, 0) + d1(M_S22, 1) + d1(M_S32, 2);
+    const CT F3 = d1(M_S13, 0) + d1(M_S32, 1) + d1(M_S33, 2);
+    const CT S11 = M[M_S11 * N + c], S12 = M[M_S12 * N + c], S13 = M[M_S13 * N + c];
+    const CT S22 = M[M_S22 * N + c], S32 = M[M_S32 * N + c], S33 = M[M_S33 * N + c];
+    const CT gam = dsqrt<CT>(CT(2)) * dsqrt<CT>(S11 * S11 + S22 * S22 + S33 * S33 + CT(2) * (S12 * S12 + S13 * S13 + S32 * S32));
+    const CT nuc = ref_cy_nu<CT>(a.nu, a.nu0, gam, a.lam, a.a, a.n);
+    F[0] += CT(2) * (nuc - a.nu) * F1;
+    F[1] += CT(2) * (nuc - a.nu) * F2;
+    F[2] += CT(2) * (nuc - a.nu) * F3;
+}
+
 // minimum resident blocks of 256 threads: the register budget of each variant (FP64
 // arithmetic and the KBC family need more live values than the cumulant in FP32)
 template <int DT, int COL>
@@ -135,124 +261,164 @@ struct StepOccupancy {
     static constexpr int value = DT == 0 ? 1 : ((COL >= COL_KBC_N1 && COL <= COL_KBC_C4) ? 2 : 3);
 };
 
+// ---------------------------------------------------------------------------------------
+// the fused step (solver/lbm3d/core.h:578-800): FLUID / PERIODIC cells collide, source
+// cells also finish their fused open-plane neighbours, self-handled nodes write their
+// equilibrium
+// ---------------------------------------------------------------------------------------
 template <int DT, int COL, bool ODD>
-__global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value) k_step(const KArgs<typename Storage<DT>::CT> a)
+__global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value) k_step(const GroupArgs<typename Storage<DT>::CT> g)
 {
     using S = Storage<DT>;
     using CT = typename S::CT;
-    using T = typename S::T;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    const bool inb = x < a.nx && y < a.ny;
-    // cell indices fit in 32 bits (nnlbm_create rejects lattices of 2^31 cells or more)
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const bool valid = warp < g.n_chunks;
+    const int4 ch = valid ? g.chunks[warp] : make_int4(0, 0, 0, 0);
+    const CaseArgs<CT>& a = g.cases[ch.z];
+    const int step = *g.cursor;
+    const int y = ch.y & 0xffff, z = ch.y >> 16;
     const int sy = a.nx, sz = a.nx * a.ny;
-    const int c = inb ? x + sy * y + sz * z : 0;
-    const int lab = inb ? (int)a.label[c] : 255;
-    const bool active = lab == L_FLUID || lab == L_PERIODIC;
-    const int flags = a.ctl[*a.cursor].flags;
-    double mass = 0.0;
-    if (active) {
+    const int x0 = ch.x - y * sy - z * sz;
+    const int x = x0 + lane;
+    const bool inb = valid && x < a.nx;
+    const int c = ch.x + lane;
+    const int raw = inb ? (int)a.label[c] : L_WALL;
+    const int lab = raw & L_MASK;
+    const bool fluid = lab == L_FLUID || lab == L_PERIODIC;
+    const bool self = (raw & LF_SELF) != 0;
+    const unsigned selfmask = __ballot_sync(0xffffffffu, self);
+    const int flags = valid ? a.ctl[step].flags : 0;
+    double mass = 0.0, qf[4] = {0.0, 0.0, 0.0, 0.0};
+    if (fluid) {
         const bool interior = x > 0 && x < a.nx - 1 && y > 0 && y < a.ny - 1 && z > 0 && z < a.nz - 1;
         CT f[27];
         if (!ODD) {
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = S::load((const T*)a.dfq[q], c, q, a.inv_scale);
+            for (int q = 0; q < 27; ++q) f[q] = S::load(qptr<DT>(a, q), c, q, a.inv_scale);
         } else {
 #pragma unroll
             for (int q = 0; q < 27; ++q) {
                 const int nb = interior ? c - (cxq(q) + sy * cyq(q) + sz * czq(q))
                                         : wrapc(x - cxq(q), a.nx) + sy * wrapc(y - cyq(q), a.ny) + sz * wrapc(z - czq(q), a.nz);
-                f[q] = S::load((const T*)a.dfq[oppq(q)], nb, q, a.inv_scale);
+                f[q] = S::load(qptr<DT>(a, oppq(q)), nb, q, a.inv_scale);
             }
         }
         CT fx = a.fx, fy = a.fy, fz = a.fz;
         if (a.cy_mode == CY_REF_FD && lab == L_FLUID) {
-            // core.h:663-781: divergence of the finite-difference strain of the previous
-            // phase with one-sided differences next to non-FLUID cells, then the CY force
-            // 2 (nu(gamma) - nu) F rho with rho still at its default of 1
-            const CT* M = a.macro;
-            const int64_t N = a.N;
-            const int cn[6] = {c - 1, c + 1, c - sy, c + sy, c - sz, c + sz};
-            bool fl[6];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) fl[k] = a.label[cn[k]] == L_FLUID;
-            auto d1 = [&](int fld, int axis) -> CT {
-                const bool m = fl[2 * axis], p = fl[2 * axis + 1];
-                const CT* F = M + (int64_t)fld * N;
-                if (!m) return p ? F[cn[2 * axis + 1]] - F[c] : CT(0);
-                if (!p) return F[c] - F[cn[2 * axis]];
-                return CT(0.5) * (F[cn[2 * axis + 1]] - F[cn[2 * axis]]);
-            };
-            const CT F1 = d1(M_S11, 0) + d1(M_S12, 1) + d1(M_S13, 2);
-            const CT F2 = d1(M_S12, 0) + d1(M_S22, 1) + d1(M_S32, 2);
-            const CT F3 = d1(M_S13, 0) + d1(M_S32, 1) + d1(M_S33, 2);
-            const CT S11 = M[M_S11 * N + c], S12 = M[M_S12 * N + c], S13 = M[M_S13 * N + c];
-            const CT S22 = M[M_S22 * N + c], S32 = M[M_S32 * N + c], S33 = M[M_S33 * N + c];
-            const CT gam = dsqrt<CT>(CT(2)) * dsqrt<CT>(S11 * S11 + S22 * S22 + S33 * S33 + CT(2) * (S12 * S12 + S13 * S13 + S32 * S32));
-            // single precision powf as in the reference
-            const CT nuc = a.nu + (a.nu0 - a.nu) * (CT)powf((float)(CT(1) + (CT)powf((float)(gam * a.lam), (float)a.a)),
-                                                           (float)((a.n - CT(1)) / a.a));
-            fx += CT(2) * (nuc - a.nu) * F1;
-            fy += CT(2) * (nuc - a.nu) * F2;
-            fz += CT(2) * (nuc - a.nu) * F3;
+            CT F[3] = {fx, fy, fz};
+            refd_force<CT>(a, c, sy, sz, F);
+            fx = F[0]; fy = F[1]; fz = F[2];
         }
         CT rho, ux, uy, uz;
         density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
+        if (raw & LF_SOURCE) {
+            // fused open-plane neighbours: their re-centred stencil is this cell's own pull
+            const StepCtl<CT>& ctl = a.ctl[step];
+            const int nbc[4] = {c - 1, c + 1, c - sy, c + sy};
+            const bool inside[4] = {x > 0, x < a.nx - 1, y > 0, y < a.ny - 1};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (!inside[k]) continue;
+                const int nr = a.label[nbc[k]];
+                const int nl = nr & L_MASK;
+                const bool ok = (nr & LF_FUSED) && (k == 0 ? nl == L_IN_L : k == 1 ? (nl == L_IN_R || nl == L_OUT_REQ)
+                                                                           : k == 2 ? nl == L_OUT_F : nl == L_OUT_B);
+                if (!ok) continue;
+                const int bx = x + (k == 0 ? -1 : k == 1 ? 1 : 0), by = y + (k == 2 ? -1 : k == 3 ? 1 : 0);
+                CT brho, bux = 0, buy = 0, buz = 0;
+                if (nl == L_IN_L || nl == L_IN_R) { // sim_tcpc.cu:242-261
+                    brho = rho;
+                    bux = nl == L_IN_L ? ctl.u_left : ctl.u_right;
+                } else { // sim_tcpc.cu:262-273, lbm_bc.h:147-152
+                    brho = CT(1); bux = ux; buy = uy; buz = uz;
+                }
+                finish_node<DT, ODD>(a, flags, nl, nbc[k], bx, by, z, brho, bux, buy, buz, qf);
+            }
+        }
         CT nu = a.nu;
         CT Sl[6];
         if (a.cy_mode == CY_LOCAL_NEQ) nu = local_nu<CT>(f, rho, ux, uy, uz, a.nu, a.nu0, a.lam, a.a, a.n, Sl);
         collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, nu);
         if (!ODD) {
 #pragma unroll
-            for (int q = 0; q < 27; ++q) S::store((T*)a.dfq[oppq(q)], c, q, f[q], a.scale);
+            for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, oppq(q)), c, q, f[q], a.scale);
         } else {
 #pragma unroll
             for (int q = 0; q < 27; ++q) {
                 const int nb = interior ? c + (cxq(q) + sy * cyq(q) + sz * czq(q))
                                         : wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz);
-                S::store((T*)a.dfq[q], nb, q, f[q], a.scale);
+                S::store(qptr<DT>(a, q), nb, q, f[q], a.scale);
             }
         }
         if ((flags & F_MACRO) || a.cy_mode == CY_REF_FD) {
-            CT* M = a.macro;
-            const int64_t N = a.N;
-            M[M_RHO * N + c] = rho; M[M_VX * N + c] = ux; M[M_VY * N + c] = uy; M[M_VZ * N + c] = uz;
-            M[M_FX * N + c] = fx; M[M_FY * N + c] = fy; M[M_FZ * N + c] = fz;
+            write_macro<CT>(a, c, rho, ux, uy, uz, fx, fy, fz);
             if (a.cy_mode == CY_LOCAL_NEQ) {
 #pragma unroll
-                for (int k = 0; k < 6; ++k) M[(M_S11 + k) * N + c] = Sl[k];
+                for (int k = 0; k < 6; ++k) a.macro[(int64_t)(M_S11 + k) * a.N + c] = Sl[k];
             }
         }
         if (flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
         if (!(rho > CT(0.25) && rho < CT(4))) atomicOr(a.err, 1);
         mass = (double)rho;
+    } else if (self) {
+        // GEO_INFLOW nodes (lbm_bc.h:126-129) and gathered open-plane nodes
+        const int k = ch.w + __popc(selfmask & ((1u << lane) - 1u));
+        CT rho, ux, uy, uz;
+        if (lab == L_IN_EQ) {
+            const StepCtl<CT>& ctl = a.ctl[step];
+            rho = ctl.rho_eq;
+            ux = g.bc_prof[3 * k] * ctl.prof_scale;
+            uy = g.bc_prof[3 * k + 1] * ctl.prof_scale;
+            uz = g.bc_prof[3 * k + 2] * ctl.prof_scale;
+        } else {
+            rho = g.bc_buf[4 * k]; ux = g.bc_buf[4 * k + 1]; uy = g.bc_buf[4 * k + 2]; uz = g.bc_buf[4 * k + 3];
+        }
+        finish_node<DT, ODD>(a, flags, lab, c, x, y, z, rho, ux, uy, uz, qf);
     }
-    if (flags & F_REDUCE) warp_add_double<CT>(mass, a.red);
+    if (flags & F_REDUCE) {
+        const double s0 = warp_sum(mass), s1 = warp_sum(qf[0]), s2 = warp_sum(qf[1]), s3 = warp_sum(qf[2]), s4 = warp_sum(qf[3]);
+        if (lane == 0) {
+            if (s0 != 0.0) atomicAdd(a.red, s0);
+            if (s1 != 0.0) atomicAdd(a.red + 1, s1);
+            if (s2 != 0.0) atomicAdd(a.red + 2, s2);
+            if (s3 != 0.0) atomicAdd(a.red + 3, s3);
+            if (s4 != 0.0) atomicAdd(a.red + 4, s4);
+        }
+    }
+    // the last block to finish advances the step cursor (every block has read it above)
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(g.done, 1) == (int)gridDim.x - 1) {
+            *g.done = 0;
+            *g.cursor = step + 1;
+            __threadfence();
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------
-// open-plane nodes
+// gathered open-plane nodes (the ones without a source neighbour)
 // ---------------------------------------------------------------------------------------
 // canonical post-collision population q of cell (x,y,z) of the previous step, in the A-A
 // layout that step left behind
 template <int DT, bool ODD>
-__device__ __forceinline__ typename Storage<DT>::CT canon(const KArgs<typename Storage<DT>::CT>& a, int x, int y, int z, int q)
+__device__ __forceinline__ typename Storage<DT>::CT canon(const CaseArgs<typename Storage<DT>::CT>& a, int x, int y, int z, int q)
 {
     using S = Storage<DT>;
-    using T = typename S::T;
     x = min(max(x, 0), a.nx - 1); y = min(max(y, 0), a.ny - 1); z = min(max(z, 0), a.nz - 1);
     const int sy = a.nx, sz = a.nx * a.ny;
     if (ODD) // the previous (even) step stored f*_q of x in slot opp(q) at x
-        return S::load((const T*)a.dfq[oppq(q)], x + sy * y + sz * z, q, a.inv_scale);
+        return S::load(qptr<DT>(a, oppq(q)), x + sy * y + sz * z, q, a.inv_scale);
     // the previous (odd) step, or the initial state, stored f*_q of x in slot q at x + c_q
-    return S::load((const T*)a.dfq[q], wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz), q,
+    return S::load(qptr<DT>(a, q), wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz), q,
                    a.inv_scale);
 }
 
 // LBM_STREAMING::streaming with explicit (m, centre, p) triples (lbm_streaming.h:10-39)
 template <int DT, bool ODD>
-__device__ __forceinline__ void pull_triples(const KArgs<typename Storage<DT>::CT>& a, const int* xs, const int* ys, const int* zs,
+__device__ __forceinline__ void pull_triples(const CaseArgs<typename Storage<DT>::CT>& a, const int* xs, const int* ys, const int* zs,
                                              typename Storage<DT>::CT* f)
 {
 #pragma unroll
@@ -260,17 +426,16 @@ __device__ __forceinline__ void pull_triples(const KArgs<typename Storage<DT>::C
 }
 
 template <int DT, bool ODD>
-__global__ void __launch_bounds__(128) k_bc_gather(const KArgs<typename Storage<DT>::CT> a)
+__global__ void __launch_bounds__(128) k_bc_gather(const GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const StepCtl<CT> ctl = a.ctl[*a.cursor];
-    if (k == 0 && (ctl.flags & F_REDUCE)) {
-        for (int i = 0; i < 5; ++i) a.red[i] = 0.0;
-    }
-    if (k >= a.n_bc) return;
-    const int c = a.bc_cell[k];
-    const int lab = a.label[c];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.n_gather) return;
+    const int4 e = g.gather[t];
+    const CaseArgs<CT>& a = g.cases[e.y];
+    const StepCtl<CT>& ctl = a.ctl[*g.cursor];
+    const int c = e.x, k = e.z;
+    const int lab = a.label[c] & L_MASK;
     const int x = c % a.nx, y = (c / a.nx) % a.ny, z = c / (a.nx * a.ny);
     // clamped neighbours of a non-periodic cell (core.h:651-661)
     const int xm = max(x - 1, 0), xp = min(x + 1, a.nx - 1), ym = max(y - 1, 0), yp = min(y + 1, a.ny - 1);
@@ -295,12 +460,6 @@ __global__ void __launch_bounds__(128) k_bc_gather(const KArgs<typename Storage<
         density_velocity<CT>(f, a.fx, a.fy, a.fz, rho, ux, uy, uz);
         rho = CT(1);
         break;
-    case L_IN_EQ: // lbm_bc.h:126-129
-        rho = ctl.rho_eq;
-        ux = a.bc_prof[3 * k] * ctl.prof_scale;
-        uy = a.bc_prof[3 * k + 1] * ctl.prof_scale;
-        uz = a.bc_prof[3 * k + 2] * ctl.prof_scale;
-        break;
     case L_OUT_REQ: // lbm_bc.h:147-152
         xs[0] = xm - 1; xs[1] = xm; xs[2] = x;
         pull_triples<DT, ODD>(a, xs, ys, zs, f);
@@ -310,67 +469,7 @@ __global__ void __launch_bounds__(128) k_bc_gather(const KArgs<typename Storage<
     default:
         break;
     }
-    a.bc_buf[4 * k] = rho; a.bc_buf[4 * k + 1] = ux; a.bc_buf[4 * k + 2] = uy; a.bc_buf[4 * k + 3] = uz;
-}
-
-template <int DT, bool ODD>
-__global__ void __launch_bounds__(128) k_bc_write(const KArgs<typename Storage<DT>::CT> a)
-{
-    using S = Storage<DT>;
-    using CT = typename S::CT;
-    using T = typename S::T;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int cur = *a.cursor;
-    const StepCtl<CT> ctl = a.ctl[cur];
-    double q3 = 0, q4 = 0, q5 = 0, q6 = 0;
-    if (k < a.n_bc) {
-        const int c = a.bc_cell[k];
-        const int lab = a.label[c];
-        const int x = c % a.nx, y = (c / a.nx) % a.ny, z = c / (a.nx * a.ny);
-        const CT rho = a.bc_buf[4 * k], ux = a.bc_buf[4 * k + 1], uy = a.bc_buf[4 * k + 2], uz = a.bc_buf[4 * k + 3];
-        CT f[27];
-        equilibrium<CT>(a.eq, rho, ux, uy, uz, f);
-        const int sy = a.nx, sz = a.nx * a.ny;
-        if (!ODD) {
-#pragma unroll
-            for (int q = 0; q < 27; ++q) S::store((T*)a.dfq[oppq(q)], c, q, f[q], a.scale);
-        } else {
-#pragma unroll
-            for (int q = 0; q < 27; ++q)
-                S::store((T*)a.dfq[q], wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz), q, f[q],
-                         a.scale);
-        }
-        if (ctl.flags & F_MACRO || a.cy_mode == CY_REF_FD) {
-            CT* M = a.macro;
-            const int64_t N = a.N;
-            M[M_RHO * N + c] = rho; M[M_VX * N + c] = ux; M[M_VY * N + c] = uy; M[M_VZ * N + c] = uz;
-            M[M_FX * N + c] = a.fx; M[M_FY * N + c] = a.fy; M[M_FZ * N + c] = a.fz;
-        }
-        if (ctl.flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
-        if (ctl.flags & F_REDUCE) {
-            if (lab == L_IN_L) q3 = (double)ux;
-            if (lab == L_IN_R) q4 = -(double)ux;
-            if (lab == L_OUT_F) q5 = -(double)uy;
-            if (lab == L_OUT_B) q6 = (double)uy;
-        }
-    }
-    if (ctl.flags & F_REDUCE) {
-        warp_add_double<CT>(q3, a.red + 1);
-        warp_add_double<CT>(q4, a.red + 2);
-        warp_add_double<CT>(q5, a.red + 3);
-        warp_add_double<CT>(q6, a.red + 4);
-    }
-    // the last block to finish advances the step cursor (every block has read it above)
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const int prev = atomicAdd(a.done, 1);
-        if (prev == (int)gridDim.x - 1) {
-            *a.done = 0;
-            *a.cursor = cur + 1;
-            __threadfence();
-        }
-    }
+    g.bc_buf[4 * k] = rho; g.bc_buf[4 * k + 1] = ux; g.bc_buf[4 * k + 2] = uy; g.bc_buf[4 * k + 3] = uz;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -379,15 +478,19 @@ __global__ void __launch_bounds__(128) k_bc_write(const KArgs<typename Storage<D
 // strain from it.  Non-FLUID values are never read by the strain stencil.
 // ---------------------------------------------------------------------------------------
 template <int DT, bool ODD>
-__global__ void __launch_bounds__(256) k_refd_velocity(const KArgs<typename Storage<DT>::CT> a)
+__global__ void __launch_bounds__(256) k_refd_velocity(const GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    if (x >= a.nx || y >= a.ny) return;
-    const int64_t c = (int64_t)x + (int64_t)a.nx * ((int64_t)y + (int64_t)a.ny * z);
-    if (a.label[c] != L_FLUID) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (warp >= g.n_chunks) return;
+    const int4 ch = g.chunks[warp];
+    const CaseArgs<CT>& a = g.cases[ch.z];
+    if (a.cy_mode != CY_REF_FD) return;
+    const int y = ch.y & 0xffff, z = ch.y >> 16;
+    const int x = ch.x - y * a.nx - z * a.nx * a.ny + lane;
+    const int c = ch.x + lane;
+    if (x >= a.nx || (a.label[c] & L_MASK) != L_FLUID) return;
     const int xs[3] = {x - 1, x, x + 1}, ys[3] = {y - 1, y, y + 1}, zs[3] = {z - 1, z, z + 1};
     CT f[27];
     pull_triples<DT, ODD>(a, xs, ys, zs, f);
@@ -399,21 +502,25 @@ __global__ void __launch_bounds__(256) k_refd_velocity(const KArgs<typename Stor
 }
 
 template <class CT>
-__global__ void __launch_bounds__(256) k_refd_stress(const KArgs<CT> a)
+__global__ void __launch_bounds__(256) k_refd_stress(const GroupArgs<CT> g)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    if (x >= a.nx || y >= a.ny) return;
-    const int64_t sy = a.nx, sz = (int64_t)a.nx * a.ny;
-    const int64_t c = (int64_t)x + sy * y + sz * z;
-    if (a.label[c] != L_FLUID) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (warp >= g.n_chunks) return;
+    const int4 ch = g.chunks[warp];
+    const CaseArgs<CT>& a = g.cases[ch.z];
+    if (a.cy_mode != CY_REF_FD) return;
+    const int sy = a.nx, sz = a.nx * a.ny;
+    const int y = ch.y & 0xffff, z = ch.y >> 16;
+    const int x = ch.x - y * sy - z * sz + lane;
+    const int c = ch.x + lane;
+    if (x >= a.nx || (a.label[c] & L_MASK) != L_FLUID) return;
     CT* M = a.macro;
     const int64_t N = a.N;
-    const int64_t cn[6] = {c - 1, c + 1, c - sy, c + sy, c - sz, c + sz};
+    const int cn[6] = {c - 1, c + 1, c - sy, c + sy, c - sz, c + sz};
     bool fl[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) fl[k] = a.label[cn[k]] == L_FLUID;
+    for (int k = 0; k < 6; ++k) fl[k] = (a.label[cn[k]] & L_MASK) == L_FLUID;
     auto d1 = [&](int fld, int axis) -> CT {
         const bool m = fl[2 * axis], p = fl[2 * axis + 1];
         const CT* F = M + (int64_t)fld * N;
@@ -434,17 +541,17 @@ __global__ void __launch_bounds__(256) k_refd_stress(const KArgs<CT> a)
 // host-side dispatch: one function per (storage, collision) instantiated in its own
 // translation unit
 // ---------------------------------------------------------------------------------------
-using StepLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args);
+using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 
 template <int DT, int COL>
 void launch_step(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<DT>::CT;
-    const KArgs<CT>& a = *(const KArgs<CT>*)args;
-    if (odd) k_step<DT, COL, true><<<grid, block, 0, s>>>(a);
-    else k_step<DT, COL, false><<<grid, block, 0, s>>>(a);
+    const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
+    if (odd) k_step<DT, COL, true><<<grid, block, 0, s>>>(g);
+    else k_step<DT, COL, false><<<grid, block, 0, s>>>(g);
 }
 
-StepLauncher step_launcher(int dtype, int collision);
+GroupLauncher step_launcher(int dtype, int collision);
 
 } // namespace nnlbm

@@ -169,7 +169,7 @@ class Lattice:
         cnt = np.zeros(5, dtype=np.int64)
         self._chk(capi.lib().nnlbm_profile_step(self.h, ic, int(n), capi.STEP_STATS if stats else 0, capi.dptr(ms),
                                                 cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
-        names = ["bc_gather", "step", "bc_write", "refd_velocity", "refd_stress"]
+        names = ["bc_gather", "step", "unused", "refd_velocity", "refd_stress"]
         return {k: (float(ms[i] / cnt[i]) if cnt[i] else 0.0, int(cnt[i])) for i, k in enumerate(names)}
 
     @property

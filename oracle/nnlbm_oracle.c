@@ -817,9 +817,11 @@ static void cell_step(orc_lattice* L, const double* src, double* dst, int x, int
         double S11 = MACRO(L, ORC_M_S11, c), S12 = MACRO(L, ORC_M_S12, c), S13 = MACRO(L, ORC_M_S13, c);
         double S22 = MACRO(L, ORC_M_S22, c), S32 = MACRO(L, ORC_M_S32, c), S33 = MACRO(L, ORC_M_S33, c);
         double gamma = sqrt(2.0) * sqrt(S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S32 * S32));
-        double nuc = nu + (d->cy_nu0 - nu) *
-                              (double)powf((float)(1.0 + (double)powf((float)(gamma * d->cy_lambda), (float)d->cy_a)),
-                                           (float)((d->cy_n - 1.0) / d->cy_a));
+        /* the reference evaluates the law with single-precision powf; here each power is
+         * taken in double and rounded once to float, i.e. the correctly rounded powf */
+        float inner = (float)pow((double)(float)(gamma * d->cy_lambda), (double)(float)d->cy_a);
+        float outer = (float)pow((double)(float)(1.0 + (double)inner), (double)(float)((d->cy_n - 1.0) / d->cy_a));
+        double nuc = nu + (d->cy_nu0 - nu) * (double)outer;
         fx += 2.0 * (nuc - nu) * F1 * 1.0;
         fy += 2.0 * (nuc - nu) * F2 * 1.0;
         fz += 2.0 * (nuc - nu) * F3 * 1.0;

@@ -196,3 +196,48 @@ def test_batched_cases_match_single():
     lat.step(25)
     for k in range(2):
         assert np.array_equal(lat.export_df(k), singles[k].export_df())
+
+
+@pytest.mark.parametrize("collision", [0, 4])
+def test_fp64_open_box_plane_corners(collision):
+    """A geometry without walls: every open plane reaches the domain edges, so plane
+    corners are gathered, and one fluid cell finishes two open-plane neighbours."""
+    wall = np.zeros((10, 12, 14), dtype=np.int32)
+    nz, ny, nx = wall.shape
+    orc = O.Oracle(nx, ny, nz, collision=collision, nu=0.05)
+    rc, counts = orc.setup_tcpc(wall)
+    lat = Lattice(CaseSpec((nx, ny, nz), collision=O.COLLISIONS[collision], dtype="f64", nu=0.05))
+    lat.setup_tcpc(wall)
+    for L in (orc, lat):
+        L.set_inflow(ivc_flux=0.02 * counts[0], svc_flux=0.01 * counts[1])
+        L.init_equilibrium()
+    for n in (1, 10, 49):
+        orc.step(n)
+        lat.step(n, macro=True, reduce=True, stats=True)
+        assert max_rel(lat.export_df(), orc.get_df(), dead_mask(orc.get_map())) <= FP64_TOL
+    r_l, r_o = lat.reduce(), orc.reduce()
+    assert np.max(np.abs(r_l[1:] - r_o[1:])) <= 1e-12
+
+
+def test_batched_mixed_groups_and_sizes():
+    """Cases of different sizes and collisions in one context: same results as alone."""
+    w1 = small_junction()
+    w2 = G.study_to_geometry(G.junction(32, 24, 20, r_ivc=5, r_svc=4, r_chamber=6, r_out=3.5, z_offset=2))
+    specs = [CaseSpec(w1.shape[::-1], dtype="f32", collision="CUM", nu=0.02),
+             CaseSpec(w2.shape[::-1], dtype="f32", collision="CUM", nu=0.03),
+             CaseSpec(w2.shape[::-1], dtype="f32", collision="BGK", nu=0.03)]
+    walls = [w1, w2, w2]
+    lat = Lattice(specs)
+    singles = [Lattice(s) for s in specs]
+    for k in range(3):
+        for L, ic in ((lat, k), (singles[k], 0)):
+            c = L.setup_tcpc(walls[k], ic=ic)
+            L.set_inflow(ivc_flux=0.03 * c["left_area"], svc_flux=0.02 * c["right_area"], ic=ic)
+    lat.init_equilibrium()
+    for s in singles:
+        s.init_equilibrium()
+        s.step(31, stats=True)
+    lat.step(31, stats=True)
+    for k in range(3):
+        assert np.array_equal(lat.export_df(k), singles[k].export_df())
+        assert np.array_equal(lat.stats(k)[0], singles[k].stats()[0])
