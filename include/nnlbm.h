@@ -124,8 +124,11 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map);
 int nnlbm_setup_tcpc(nnlbm_ctx* ctx, int ic, const int32_t* wall, int64_t* counts);
 
 /* The same boundary setup without a context or a device (host only): map_out [nz][ny][nx]
- * solver labels, counts as above. */
-int nnlbm_tcpc_labels(int32_t nx, int32_t ny, int32_t nz, const int32_t* wall, uint8_t* map_out, int64_t* counts);
+ * solver labels, wall_flags_out (may be NULL) the wall flags after the planes were opened
+ * (LBM::getWall, read by the output's near-wall test, sim_tcpc.cu:709-714), counts as
+ * above. */
+int nnlbm_tcpc_labels(int32_t nx, int32_t ny, int32_t nz, const int32_t* wall, uint8_t* map_out,
+                      uint8_t* wall_flags_out, int64_t* counts);
 
 /* Replaces: resetLattice / setEqLat + LBMKernelInit (sim_tcpc.cu:647-655,
  * lbm.hpp:1-39, core.h:833-863). */
@@ -153,7 +156,8 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags);
 /* Replaces: StateTcpc::statReset (sim_tcpc.cu:665-682). */
 int nnlbm_stat_reset(nnlbm_ctx* ctx, int ic);
 
-/* Macro field of the last step that had NNLBM_STEP_MACRO; out: [nz][ny][nx] doubles.
+/* Macro field of the last step that had NNLBM_STEP_MACRO (before any such step: the
+ * initial state of LBMKernelInit, core.h:833-863); out: [nz][ny][nx] doubles.
  * Replaces: LBM::copyMacroToHost (core.h:1334). */
 int nnlbm_get_macro(nnlbm_ctx* ctx, int ic, int field, double* out);
 

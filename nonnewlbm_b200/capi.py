@@ -84,7 +84,7 @@ def lib():
         L.nnlbm_stream.restype = _vp
         L.nnlbm_last_error.argtypes = [_vp, ctypes.c_char_p, ctypes.c_size_t]
         L.nnlbm_destroy.argtypes = [_vp]
-        L.nnlbm_tcpc_labels.argtypes = [ctypes.c_int32] * 3 + [_vp, _vp, _vp]
+        L.nnlbm_tcpc_labels.argtypes = [ctypes.c_int32] * 3 + [_vp, _vp, _vp, _vp]
         _lib = L
     return _lib
 
@@ -104,15 +104,17 @@ def check(h, rc: int) -> None:
         raise NnlbmError(rc, last_error(h))
 
 
-def tcpc_labels(wall: np.ndarray):
+def tcpc_labels(wall: np.ndarray, with_wall_flags: bool = False):
     """Host-only TCPC boundary setup (nnlbm_tcpc_labels): geometry wall array [z][y][x] ->
-    (solver map, counts dict, status)."""
+    (solver map, counts dict, status[, wall flags])."""
     w = np.ascontiguousarray(wall, dtype=np.int32)
     nz, ny, nx = w.shape
     m = np.zeros(w.shape, dtype=np.uint8)
+    wf = np.zeros(w.shape, dtype=np.uint8)
     counts = np.zeros(10, dtype=np.int64)
-    rc = lib().nnlbm_tcpc_labels(nx, ny, nz, w.ctypes.data, m.ctypes.data, counts.ctypes.data)
+    rc = lib().nnlbm_tcpc_labels(nx, ny, nz, w.ctypes.data, m.ctypes.data, wf.ctypes.data, counts.ctypes.data)
     if rc not in (OK, ERR_AREA):
         raise NnlbmError(rc, "invalid TCPC geometry")
     keys = ["left_area", "right_area", "outlet5", "outlet6", "wall", "fluid", "vtk3", "vtk4", "vtk5", "vtk6"]
-    return m, dict(zip(keys, (int(v) for v in counts))), rc
+    out = (m, dict(zip(keys, (int(v) for v in counts))), rc)
+    return out + (wf.astype(bool),) if with_wall_flags else out

@@ -93,6 +93,7 @@ struct Case {
     int64_t iterations = 0;
     int64_t n_stats = 0;
     bool has_map = false, has_state = false;
+    double init[4] = {1.0, 0.0, 0.0, 0.0}; // rho, u of the last initial equilibrium
     std::vector<char> args;          // CaseArgs<CT>
 };
 
@@ -191,7 +192,7 @@ int ensure_macro(nnlbm_ctx* ctx, Case& c)
     if (c.d_macro) return NNLBM_OK;
     CK(cudaMalloc(&c.d_macro, (size_t)M_N * c.N * c.ct_bytes));
     rebuild_case_args(ctx, c);
-    aux_launchers(c.d.dtype).init_macro(c.args.data(), 1.0, 0.0, 0.0, 0.0, ctx->stream);
+    aux_launchers(c.d.dtype).init_macro(c.args.data(), c.init[0], c.init[1], c.init[2], c.init[3], ctx->stream);
     CK(cudaGetLastError());
     return NNLBM_OK;
 }
@@ -612,7 +613,8 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
 }
 
 // StateTcpc::setupBoundaries (sim_tcpc.cu:494-645) + LBM::projectWall (lbm.hpp:144-155)
-int nnlbm_tcpc_labels(int32_t X, int32_t Y, int32_t Z, const int32_t* wall, uint8_t* map_out, int64_t* counts)
+int nnlbm_tcpc_labels(int32_t X, int32_t Y, int32_t Z, const int32_t* wall, uint8_t* map_out, uint8_t* wall_flags_out,
+                      int64_t* counts)
 {
     if (X < 3 || Y < 3 || Z < 3 || !wall || !map_out) return NNLBM_ERR_ARG;
     const size_t N = (size_t)X * Y * Z;
@@ -667,6 +669,7 @@ int nnlbm_tcpc_labels(int32_t X, int32_t Y, int32_t Z, const int32_t* wall, uint
     }
     for (size_t i = 0; i < N; ++i)
         if (wf[i]) map[i] = L_WALL;
+    if (wall_flags_out) memcpy(wall_flags_out, wf.data(), N);
     if (counts) {
         const int64_t v[10] = {la, ra, of, ob, wc, fc, in[3], in[4], in[5], in[6]};
         memcpy(counts, v, sizeof v);
@@ -682,7 +685,7 @@ int nnlbm_setup_tcpc(nnlbm_ctx* ctx, int ic, const int32_t* wall, int64_t* count
     Case& c = ctx->cases[ic];
     std::vector<uint8_t> map((size_t)c.N);
     int64_t cnt[10];
-    const int lrc = nnlbm_tcpc_labels(c.d.nx, c.d.ny, c.d.nz, wall, map.data(), cnt);
+    const int lrc = nnlbm_tcpc_labels(c.d.nx, c.d.ny, c.d.nz, wall, map.data(), nullptr, cnt);
     if (counts) memcpy(counts, cnt, sizeof cnt);
     if ((rc = nnlbm_set_map(ctx, ic, map.data())) != NNLBM_OK) return rc;
     if (lrc == NNLBM_ERR_AREA)
@@ -706,6 +709,7 @@ int nnlbm_init_equilibrium(nnlbm_ctx* ctx, int ic, double rho, double ux, double
     CK(cudaMemsetAsync(c.d_err, 0, sizeof(int), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     c.parity = 0; c.iterations = 0; c.n_stats = 0;
+    c.init[0] = rho; c.init[1] = ux; c.init[2] = uy; c.init[3] = uz;
     c.has_state = true;
     return NNLBM_OK;
 }
@@ -786,8 +790,11 @@ int nnlbm_get_macro(nnlbm_ctx* ctx, int ic, int field, double* out)
     if (rc) return rc;
     if (field < 0 || field >= M_N || !out) return set_err(ctx, NNLBM_ERR_ARG, "bad macro field %d", field);
     Case& c = ctx->cases[ic];
-    if (!c.d_macro) return set_err(ctx, NNLBM_ERR_ARG, "no macro state yet: run a step with NNLBM_STEP_MACRO");
     CK(cudaSetDevice(ctx->device));
+    if (!c.d_macro) { // the initial state (LBMKernelInit, core.h:833-863)
+        if ((rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     if (c.ct_bytes == 8) {
         CK(cudaMemcpy(out, (char*)c.d_macro + (size_t)field * c.N * 8, (size_t)c.N * 8, cudaMemcpyDeviceToHost));
     } else {
