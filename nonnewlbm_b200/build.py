@@ -58,17 +58,21 @@ def _stale(obj: Path, deps) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, jobs: int | None = None, verbose: bool = False, ptxas_info: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False, ptxas_info: bool = False,
+          out: Path | None = None, build_dir: Path | None = None, defines=()) -> Path:
+    """Compile every translation unit (skipping up-to-date objects) and link ``out``."""
+    lib_path = Path(out) if out else LIB
+    bdir = Path(build_dir) if build_dir else BUILD
+    bdir.mkdir(parents=True, exist_ok=True)
     cc = nvcc()
     jobs = jobs or max(1, os.cpu_count() or 1)
     todo = []
     objs = []
     for name, src, extra, hdrs in units():
-        obj = BUILD / f"{name}.o"
+        obj = bdir / f"{name}.o"
         objs.append(obj)
         if force or _stale(obj, [src, *hdrs, Path(__file__)]):
-            cmd = [cc, *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
+            cmd = [cc, *ARCH, *COMMON, *extra, *[f"-D{d}" for d in defines], "-c", str(src), "-o", str(obj)]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             todo.append((name, cmd))
@@ -88,12 +92,12 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False, p
                     failed.append(name)
     if failed:
         raise RuntimeError(f"nvcc failed for {failed}")
-    if todo or force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    if todo or force or not lib_path.exists() or any(o.stat().st_mtime > lib_path.stat().st_mtime for o in objs):
+        tmp = lib_path.with_suffix(".so.tmp")
         cmd = [cc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
         subprocess.check_call(cmd)
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib_path)
+    return lib_path
 
 
 def main() -> int:

@@ -290,6 +290,8 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     g.args.resize(sizeof(GroupArgs<CT>));
     GroupArgs<CT>& ga = *(GroupArgs<CT>*)g.args.data();
     memset(&ga, 0, sizeof ga);
+    ga.c0 = ca[0];
+    ga.n_cases = (int)ca.size();
     ga.cases = (const CaseArgs<CT>*)g.d_cases;
     ga.chunks = g.d_chunks;
     ga.n_chunks = g.n_chunks;

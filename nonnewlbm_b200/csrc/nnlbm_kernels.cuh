@@ -105,6 +105,8 @@ struct CaseArgs {
 // a launch group: cases sharing storage type and collision
 template <class CT>
 struct GroupArgs {
+    CaseArgs<CT> c0;           // copy of case 0 in parameter space (single-case groups)
+    int n_cases, pad2;
     const CaseArgs<CT>* cases;
     const int4* chunks;        // {first cell, y | z << 16, case, first self-node index}
     int n_chunks, pad0;
@@ -198,29 +200,25 @@ __device__ __forceinline__ void store_node_eq(const CaseArgs<typename Storage<DT
     }
 }
 
-// macro / stats / flux bookkeeping of an open-plane node
+// macro / stats bookkeeping of an open-plane node; returns its contribution to the plane
+// flux sums of postprocess/compute_flows.py:107-147 (inflow positive at 3/4)
 template <class CT>
-__device__ __forceinline__ void node_outputs(const CaseArgs<CT>& a, int flags, int lab, int c, CT rho, CT ux, CT uy, CT uz,
-                                             double* qf)
+__device__ __forceinline__ double node_outputs(const CaseArgs<CT>& a, int flags, int lab, int c, CT rho, CT ux, CT uy, CT uz)
 {
     if ((flags & F_MACRO) || a.cy_mode == CY_REF_FD) write_macro<CT>(a, c, rho, ux, uy, uz, a.fx, a.fy, a.fz);
     if (flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
-    // plane fluxes of postprocess/compute_flows.py:107-147, inflow positive at 3/4
-    if (lab == L_IN_L) qf[0] += (double)ux;
-    if (lab == L_IN_R) qf[1] -= (double)ux;
-    if (lab == L_OUT_F) qf[2] -= (double)uy;
-    if (lab == L_OUT_B) qf[3] += (double)uy;
+    return lab == L_IN_L ? (double)ux : lab == L_IN_R ? -(double)ux : lab == L_OUT_F ? -(double)uy : lab == L_OUT_B ? (double)uy : 0.0;
 }
 
 // rare paths of the step kernel are kept out of line so that they do not take registers
 // from the bulk path: the equilibrium of an open-plane node with its bookkeeping ...
 template <int DT, bool ODD>
-__device__ __noinline__ void finish_node(const CaseArgs<typename Storage<DT>::CT>& a, int flags, int lab, int c, int x, int y, int z,
-                                         typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
-                                         typename Storage<DT>::CT uy, typename Storage<DT>::CT uz, double* qf)
+__device__ __noinline__ double finish_node(const CaseArgs<typename Storage<DT>::CT>& a, int flags, int lab, int c, int x, int y,
+                                           int z, typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
+                                           typename Storage<DT>::CT uy, typename Storage<DT>::CT uz)
 {
     store_node_eq<DT, ODD>(a, c, x, y, z, rho, ux, uy, uz);
-    node_outputs<typename Storage<DT>::CT>(a, flags, lab, c, rho, ux, uy, uz, qf);
+    return node_outputs<typename Storage<DT>::CT>(a, flags, lab, c, rho, ux, uy, uz);
 }
 
 // ... and the finite-difference Carreau-Yasuda force of CY_REF_FD (core.h:663-781):
@@ -256,9 +254,12 @@ __device__ __noinline__ void refd_force(const CaseArgs<CT>& a, int c, int sy, in
 
 // minimum resident blocks of 256 threads: the register budget of each variant (FP64
 // arithmetic and the KBC family need more live values than the cumulant in FP32)
+#ifndef NNLBM_STEP_MINB
+#define NNLBM_STEP_MINB 3
+#endif
 template <int DT, int COL>
 struct StepOccupancy {
-    static constexpr int value = DT == 0 ? 1 : ((COL >= COL_KBC_N1 && COL <= COL_KBC_C4) ? 2 : 3);
+    static constexpr int value = DT == 0 ? 1 : ((COL >= COL_KBC_N1 && COL <= COL_KBC_C4) ? 2 : NNLBM_STEP_MINB);
 };
 
 // ---------------------------------------------------------------------------------------
@@ -266,8 +267,9 @@ struct StepOccupancy {
 // cells also finish their fused open-plane neighbours, self-handled nodes write their
 // equilibrium
 // ---------------------------------------------------------------------------------------
-template <int DT, int COL, bool ODD>
-__global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value) k_step(const GroupArgs<typename Storage<DT>::CT> g)
+template <int DT, int COL, bool ODD, bool SINGLE>
+__global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
+    k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using S = Storage<DT>;
     using CT = typename S::CT;
@@ -275,7 +277,8 @@ __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value) k_step(con
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const bool valid = warp < g.n_chunks;
     const int4 ch = valid ? g.chunks[warp] : make_int4(0, 0, 0, 0);
-    const CaseArgs<CT>& a = g.cases[ch.z];
+    // a single-case group reads its parameters from the constant bank
+    const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[ch.z];
     const int step = *g.cursor;
     const int y = ch.y & 0xffff, z = ch.y >> 16;
     const int sy = a.nx, sz = a.nx * a.ny;
@@ -289,7 +292,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value) k_step(con
     const bool self = (raw & LF_SELF) != 0;
     const unsigned selfmask = __ballot_sync(0xffffffffu, self);
     const int flags = valid ? a.ctl[step].flags : 0;
-    double mass = 0.0, qf[4] = {0.0, 0.0, 0.0, 0.0};
+    double mass = 0.0, q3 = 0.0, q4 = 0.0, q5 = 0.0, q6 = 0.0;
     if (fluid) {
         const bool interior = x > 0 && x < a.nx - 1 && y > 0 && y < a.ny - 1 && z > 0 && z < a.nz - 1;
         CT f[27];
@@ -333,13 +336,20 @@ __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value) k_step(con
                 } else { // sim_tcpc.cu:262-273, lbm_bc.h:147-152
                     brho = CT(1); bux = ux; buy = uy; buz = uz;
                 }
-                finish_node<DT, ODD>(a, flags, nl, nbc[k], bx, by, z, brho, bux, buy, buz, qf);
+                const double qn = finish_node<DT, ODD>(a, flags, nl, nbc[k], bx, by, z, brho, bux, buy, buz);
+                if (nl == L_IN_L) q3 += qn;
+                else if (nl == L_IN_R) q4 += qn;
+                else if (nl == L_OUT_F) q5 += qn;
+                else if (nl == L_OUT_B) q6 += qn;
             }
         }
-        CT nu = a.nu;
         CT Sl[6];
-        if (a.cy_mode == CY_LOCAL_NEQ) nu = local_nu<CT>(f, rho, ux, uy, uz, a.nu, a.nu0, a.lam, a.a, a.n, Sl);
-        collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, nu);
+        if (a.cy_mode == CY_LOCAL_NEQ) {
+            const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
+            collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu, &cy, Sl);
+        } else {
+            collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu);
+        }
         if (!ODD) {
 #pragma unroll
             for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, oppq(q)), c, q, f[q], a.scale);
@@ -374,10 +384,14 @@ __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value) k_step(con
         } else {
             rho = g.bc_buf[4 * k]; ux = g.bc_buf[4 * k + 1]; uy = g.bc_buf[4 * k + 2]; uz = g.bc_buf[4 * k + 3];
         }
-        finish_node<DT, ODD>(a, flags, lab, c, x, y, z, rho, ux, uy, uz, qf);
+        const double qn = finish_node<DT, ODD>(a, flags, lab, c, x, y, z, rho, ux, uy, uz);
+        if (lab == L_IN_L) q3 = qn;
+        else if (lab == L_IN_R) q4 = qn;
+        else if (lab == L_OUT_F) q5 = qn;
+        else if (lab == L_OUT_B) q6 = qn;
     }
     if (flags & F_REDUCE) {
-        const double s0 = warp_sum(mass), s1 = warp_sum(qf[0]), s2 = warp_sum(qf[1]), s3 = warp_sum(qf[2]), s4 = warp_sum(qf[3]);
+        const double s0 = warp_sum(mass), s1 = warp_sum(q3), s2 = warp_sum(q4), s3 = warp_sum(q5), s4 = warp_sum(q6);
         if (lane == 0) {
             if (s0 != 0.0) atomicAdd(a.red, s0);
             if (s1 != 0.0) atomicAdd(a.red + 1, s1);
@@ -426,7 +440,7 @@ __device__ __forceinline__ void pull_triples(const CaseArgs<typename Storage<DT>
 }
 
 template <int DT, bool ODD>
-__global__ void __launch_bounds__(128) k_bc_gather(const GroupArgs<typename Storage<DT>::CT> g)
+__global__ void __launch_bounds__(128) k_bc_gather(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -478,7 +492,7 @@ __global__ void __launch_bounds__(128) k_bc_gather(const GroupArgs<typename Stor
 // strain from it.  Non-FLUID values are never read by the strain stencil.
 // ---------------------------------------------------------------------------------------
 template <int DT, bool ODD>
-__global__ void __launch_bounds__(256) k_refd_velocity(const GroupArgs<typename Storage<DT>::CT> g)
+__global__ void __launch_bounds__(256) k_refd_velocity(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
     const int lane = threadIdx.x & 31;
@@ -502,7 +516,7 @@ __global__ void __launch_bounds__(256) k_refd_velocity(const GroupArgs<typename 
 }
 
 template <class CT>
-__global__ void __launch_bounds__(256) k_refd_stress(const GroupArgs<CT> g)
+__global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ GroupArgs<CT> g)
 {
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -548,8 +562,13 @@ void launch_step(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* ar
 {
     using CT = typename Storage<DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
-    if (odd) k_step<DT, COL, true><<<grid, block, 0, s>>>(g);
-    else k_step<DT, COL, false><<<grid, block, 0, s>>>(g);
+    if (g.n_cases == 1) {
+        if (odd) k_step<DT, COL, true, true><<<grid, block, 0, s>>>(g);
+        else k_step<DT, COL, false, true><<<grid, block, 0, s>>>(g);
+    } else {
+        if (odd) k_step<DT, COL, true, false><<<grid, block, 0, s>>>(g);
+        else k_step<DT, COL, false, false><<<grid, block, 0, s>>>(g);
+    }
 }
 
 GroupLauncher step_launcher(int dtype, int collision);

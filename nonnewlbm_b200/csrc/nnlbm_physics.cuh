@@ -151,7 +151,17 @@ __device__ __forceinline__ void bwd3(CT k0, CT k1, CT k2, CT u, CT& m, CT& z, CT
 }
 
 template <class CT>
-__device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu)
+struct CYParams;
+template <class CT>
+__device__ __forceinline__ CT cy_nu_from_central(CT Cxx, CT Cyy, CT Czz, CT Cxy, CT Cxz, CT Cyz, CT rho, const CYParams<CT>& p,
+                                                 CT* S);
+
+// `cy` non-null: the shear viscosity comes from the Carreau-Yasuda law evaluated on this
+// cell's own central second moments (k_200 ... k_011 of the forward transform); S receives
+// the strain rate
+template <class CT>
+__device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu, const CYParams<CT>* cy = nullptr,
+                                            CT* S = nullptr)
 {
     // forward: z pass over the 9 (x,y) columns
     CT a[3][3][3];
@@ -176,6 +186,7 @@ __device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, 
             if (ky + kz <= 2) fwd3<CT>(b[0][ky][kz], b[1][ky][kz], b[2][ky][kz], ux, k[0][ky][kz], k[1][ky][kz], k[2][ky][kz]);
 
     const CT ir = CT(1) / rho;
+    if (cy) nu = cy_nu_from_central<CT>(k[2][0][0], k[0][2][0], k[0][0][2], k[1][1][0], k[1][0][1], k[0][1][1], rho, *cy, S);
     const CT om = CT(1) / (CT(3) * nu + CT(0.5));
     const CT k000 = k[0][0][0];
     // relaxation (lbm_col_cum.h:205-235 with omega2 = 1 and no anti-aliasing terms)
@@ -409,10 +420,18 @@ __device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, 
     }
 }
 
+template <class CT>
+__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, const CYParams<CT>& p, CT* S);
+
+// one collision; with `cy` the shear viscosity is the local Carreau-Yasuda one
 template <class CT, int COL>
-__device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz, CT nu)
+__device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz, CT nu,
+                                        const CYParams<CT>* cy = nullptr, CT* S = nullptr)
 {
-    if constexpr (COL == COL_CUM) collide_cum<CT>(f, rho, ux, uy, uz, nu);
+    if constexpr (COL != COL_CUM) {
+        if (cy) nu = local_nu<CT>(f, rho, ux, uy, uz, *cy, S);
+    }
+    if constexpr (COL == COL_CUM) collide_cum<CT>(f, rho, ux, uy, uz, nu, cy, S);
     else if constexpr (COL == COL_MRT) collide_mrt<CT>(f, rho, ux, uy, uz, nu);
     else if constexpr (COL == COL_BGK) collide_bgk<CT>(f, rho, ux, uy, uz, fx, fy, fz, nu);
     else {
@@ -430,29 +449,27 @@ __device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT f
 // The viscosity law is the reference's (solver/lbm3d/core.h:763-766).
 // ---------------------------------------------------------------------------------------
 template <class CT>
-__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, CT nu_inf, CT nu0, CT lam, CT a, CT n, CT* S)
+struct CYParams { CT nu_inf, nu0, lam, a, n; };
+
+// from the central second moments Cxx.. (not yet reduced by rho/3 on the diagonal)
+template <class CT>
+__device__ __forceinline__ CT cy_nu_from_central(CT Cxx, CT Cyy, CT Czz, CT Cxy, CT Cxz, CT Cyz, CT rho, const CYParams<CT>& p,
+                                                 CT* S)
 {
-    CT Cxx = 0, Cyy = 0, Czz = 0, Cxy = 0, Cxz = 0, Cyz = 0;
-#pragma unroll
-    for (int q = 0; q < 27; ++q) {
-        const CT dx = CT(cxq(q)) - ux, dy = CT(cyq(q)) - uy, dz = CT(czq(q)) - uz, v = f[q];
-        Cxx += dx * dx * v; Cyy += dy * dy * v; Czz += dz * dz * v;
-        Cxy += dx * dy * v; Cxz += dx * dz * v; Cyz += dy * dz * v;
-    }
     const CT Pxx = Cxx - rho * CT(1.0 / 3.0), Pyy = Cyy - rho * CT(1.0 / 3.0), Pzz = Czz - rho * CT(1.0 / 3.0);
     const CT pn = dsqrt<CT>(Pxx * Pxx + Pyy * Pyy + Pzz * Pzz + CT(2) * (Cxy * Cxy + Cxz * Cxz + Cyz * Cyz));
     const CT K = CT(3) * CT(1.4142135623730951) * pn / (CT(2) * rho);
-    CT tau = CT(3) * nu0 + CT(0.5);
+    CT tau = CT(3) * p.nu0 + CT(0.5);
     if (K > CT(0)) {
-        const CT e = (n - CT(1)) / a;
+        const CT e = (p.n - CT(1)) / p.a;
 #pragma unroll
         for (int it = 0; it < 3; ++it) {
             const CT g = K / tau;
-            const CT s = dpow<CT>(lam * g, a);
-            const CT p = dpow<CT>(CT(1) + s, e);
-            const CT nuc = nu_inf + (nu0 - nu_inf) * p;
+            const CT s = dpow<CT>(p.lam * g, p.a);
+            const CT pw = dpow<CT>(CT(1) + s, e);
+            const CT nuc = p.nu_inf + (p.nu0 - p.nu_inf) * pw;
             const CT G = tau - CT(3) * nuc - CT(0.5);
-            const CT gdn = (nu0 - nu_inf) * (n - CT(1)) * s * p / (CT(1) + s);
+            const CT gdn = (p.nu0 - p.nu_inf) * (p.n - CT(1)) * s * pw / (CT(1) + s);
             const CT Gp = CT(1) + CT(3) * gdn / tau;
             tau = tau - G / Gp;
         }
@@ -460,6 +477,32 @@ __device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz,
     const CT sc = CT(-3) / (CT(2) * rho * tau);
     S[0] = sc * Pxx; S[1] = sc * Cxy; S[2] = sc * Cxz; S[3] = sc * Pyy; S[4] = sc * Cyz; S[5] = sc * Pzz;
     return (tau - CT(0.5)) * CT(1.0 / 3.0);
+}
+
+// the same from the populations: raw second moments by additions only (c in {-1,0,1}),
+// shifted to central ones with the raw momentum j: C_ab = M_ab - u_a j_b - u_b j_a + rho u_a u_b
+template <class CT>
+__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, const CYParams<CT>& p, CT* S)
+{
+    CT Mxx = 0, Myy = 0, Mzz = 0, Mxy = 0, Mxz = 0, Myz = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const int cx = cxq(q), cy = cyq(q), cz = czq(q);
+        const CT v = f[q];
+        if (cx) { Mxx += v; if (cx > 0) jx += v; else jx -= v; }
+        if (cy) { Myy += v; if (cy > 0) jy += v; else jy -= v; }
+        if (cz) { Mzz += v; if (cz > 0) jz += v; else jz -= v; }
+        if (cx * cy > 0) Mxy += v; else if (cx * cy < 0) Mxy -= v;
+        if (cx * cz > 0) Mxz += v; else if (cx * cz < 0) Mxz -= v;
+        if (cy * cz > 0) Myz += v; else if (cy * cz < 0) Myz -= v;
+    }
+    const CT Cxx = Mxx - CT(2) * ux * jx + rho * ux * ux;
+    const CT Cyy = Myy - CT(2) * uy * jy + rho * uy * uy;
+    const CT Czz = Mzz - CT(2) * uz * jz + rho * uz * uz;
+    const CT Cxy = Mxy - ux * jy - uy * jx + rho * ux * uy;
+    const CT Cxz = Mxz - ux * jz - uz * jx + rho * ux * uz;
+    const CT Cyz = Myz - uy * jz - uz * jy + rho * uy * uz;
+    return cy_nu_from_central<CT>(Cxx, Cyy, Czz, Cxy, Cxz, Cyz, rho, p, S);
 }
 
 } // namespace nnlbm
