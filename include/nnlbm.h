@@ -153,6 +153,39 @@ int nnlbm_set_schedule(nnlbm_ctx* ctx, int ic, const double* rows, int64_t n);
  * applied to every step; NNLBM_STEP_MACRO and NNLBM_STEP_REDUCE apply to the last step. */
 int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags);
 
+/* Size of the one scratch array that nnlbm_step_noalloc uses on each device: two step
+ * counters (256 bytes) plus, per launch group, four values (rho, ux, uy, uz) of the
+ * arithmetic type for each open-plane node that its own thread writes (nnlbm_step_info's
+ * bc_cells bounds that count).  4 MiB holds 262,128 such nodes in FP32 arithmetic and
+ * 131,064 in FP64. */
+#define NNLBM_NOALLOC_SCRATCH_BYTES (4u << 20)
+
+/* nnlbm_step that allocates no device memory.  No counterpart in the reference (its
+ * sim_tcpc allocates every buffer at start-up and owns the whole device).
+ *
+ * It is meant for callers that cannot allocate while they step: a host loop that shares
+ * the GPU with work on other streams (cudaMalloc and cudaFree synchronise the device and
+ * would stall that work), and a coupled solver that reserved its HBM budget up front and
+ * must not meet an out-of-memory error in the middle of a run.
+ *
+ * Same kernels, arguments and results as nnlbm_step, run as plain launches (no CUDA
+ * graph).  The per-call scratch of nnlbm_step (the step cursor, the block counter and the
+ * gathered open-plane node values) lives instead in one file-scope device array of
+ * NNLBM_NOALLOC_SCRATCH_BYTES per device.  Its address is looked up the first time this
+ * function runs on a device (cudaGetSymbolAddress, with the device current), so that
+ * first call should come before any stream capture.  Every call shares the array: the
+ * counters are cleared at the start of each group's steps (the node values are written
+ * before they are read in every step and need no clearing), and calls that overlap in
+ * time, from two contexts on one device or from two host threads, race on it.
+ *
+ * It returns NNLBM_ERR_ARG, with a message, and launches nothing when a buffer would
+ * have to be allocated first: a launch group whose work lists are not on the device yet
+ * (call nnlbm_step or nnlbm_step_info once after nnlbm_set_map / nnlbm_setup_tcpc),
+ * NNLBM_STEP_MACRO or NNLBM_STEP_STATS (or NNLBM_CY_REF_FD) before any nnlbm_step with
+ * that flag, n_steps above the control rows in place (at least 1024), or more
+ * open-plane nodes than the scratch array holds. */
+int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags);
+
 /* Replaces: StateTcpc::statReset (sim_tcpc.cu:665-682). */
 int nnlbm_stat_reset(nnlbm_ctx* ctx, int ic);
 

@@ -26,7 +26,7 @@ M_RHO, M_VX, M_VY, M_VZ, M_FX, M_FY, M_FZ, M_S11, M_S12, M_S13, M_S22, M_S32, M_
 
 EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
-    "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_stat_reset", "nnlbm_get_macro",
+    "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_step_noalloc", "nnlbm_stat_reset", "nnlbm_get_macro",
     "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_step_info", "nnlbm_profile_step",
     "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels",
 ]
@@ -71,6 +71,7 @@ def lib():
         L.nnlbm_set_inflow_profile.argtypes = [_vp, i, _dp, ctypes.c_int64]
         L.nnlbm_set_schedule.argtypes = [_vp, i, _dp, ctypes.c_int64]
         L.nnlbm_step.argtypes = [_vp, ctypes.c_int64, i]
+        L.nnlbm_step_noalloc.argtypes = [_vp, ctypes.c_int64, i]
         L.nnlbm_stat_reset.argtypes = [_vp, i]
         L.nnlbm_get_macro.argtypes = [_vp, i, i, _dp]
         L.nnlbm_get_stats.argtypes = [_vp, i, _dp, _i64p]

@@ -10,6 +10,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -450,6 +451,82 @@ size_t canon_index(const Case& c, int x, int y, int z, int q, int* slot)
     *slot = q; // after an odd step (or the initial state): slot q at x + c_q
     const int xx = (x + cxq(q) + nx) % nx, yy = (y + cyq(q) + ny) % ny, zz = (z + czq(q) + nz) % nz;
     return (size_t)xx + (size_t)nx * (yy + (size_t)ny * zz);
+}
+
+// ---------------------------------------------------------------------------------------
+// scratch of nnlbm_step_noalloc: one file-scope device array per device (the module's
+// global), never allocated or freed by this library.  Layout: [0, 256) the step cursor and
+// the block counter of the step kernel, then the gathered open-plane node values
+// (rho, ux, uy, uz per node) of the launch group being stepped.
+// ---------------------------------------------------------------------------------------
+constexpr size_t kNoallocHead = 256;
+constexpr int kNoallocDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoallocDevices] = {};
+
+} // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NNLBM_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+// device address of the scratch array on the context's device, looked up once per device
+// with that device current (the caller has made it current)
+int noalloc_scratch(nnlbm_ctx* ctx, char** out)
+{
+    if (ctx->device < 0 || ctx->device >= kNoallocDevices)
+        return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: device %d beyond the %d supported", ctx->device,
+                       kNoallocDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[ctx->device]) {
+        void* p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[ctx->device] = p;
+    }
+    *out = (char*)g_noalloc_ptr[ctx->device];
+    return NNLBM_OK;
+}
+
+// the control rows of fill_ctl, staged through a fixed host buffer (no allocation)
+template <class CT>
+int upload_ctl_rows(nnlbm_ctx* ctx, const Case& c, int64_t n, int flags)
+{
+    constexpr int kRows = 64;
+    StepCtl<CT> r[kRows];
+    const int64_t ns = (int64_t)c.sched.size() / 3;
+    for (int64_t k0 = 0; k0 < n; k0 += kRows) {
+        const int cnt = (int)std::min<int64_t>(kRows, n - k0);
+        for (int j = 0; j < cnt; ++j) {
+            const int64_t k = k0 + j;
+            double ivc = c.ivc_flux, svc = c.svc_flux, ps = 1.0;
+            if (ns > 0) {
+                const int64_t t = std::min(k, ns - 1);
+                ivc = c.sched[3 * t]; svc = c.sched[3 * t + 1]; ps = c.sched[3 * t + 2];
+            }
+            int f = flags & NNLBM_STEP_STATS;
+            if (k == n - 1) f |= flags & (NNLBM_STEP_MACRO | NNLBM_STEP_REDUCE);
+            r[j].flags = f;
+            r[j].pad = 0;
+            r[j].u_left = c.left_area > 0 ? (CT)ivc / (CT)c.left_area : CT(0);
+            r[j].u_right = c.right_area > 0 ? (CT)(-svc) / (CT)c.right_area : CT(0);
+            r[j].rho_left = (CT)c.rho_left; r[j].rho_right = (CT)c.rho_right; r[j].rho_eq = (CT)c.rho_eq;
+            r[j].prof_scale = (CT)ps;
+        }
+        // pageable source: the call returns once the rows have been staged, so r is reusable
+        CK(cudaMemcpyAsync((StepCtl<CT>*)c.d_ctl + k0, r, cnt * sizeof(StepCtl<CT>), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return NNLBM_OK;
+}
+
+// the group's kernel arguments with the per-call scratch moved into the static array
+template <class CT>
+void noalloc_args(const Group& g, char* scratch, char* out)
+{
+    GroupArgs<CT>& ga = *(GroupArgs<CT>*)out;
+    memcpy(&ga, g.args.data(), sizeof ga);
+    ga.cursor = (int*)scratch;
+    ga.done = (int*)scratch + 1;
+    ga.bc_buf = (CT*)(scratch + kNoallocHead);
 }
 
 } // namespace
@@ -1016,6 +1093,100 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
     }
     for (auto& e : ev) cudaEventDestroy(e);
     finish_steps(ctx, g, n_steps, flags);
+    return NNLBM_OK;
+}
+
+int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
+{
+    if (!ctx) return NNLBM_ERR_ARG;
+    if (n_steps < 0) return set_err(ctx, NNLBM_ERR_ARG, "negative step count");
+    if (n_steps == 0) return NNLBM_OK;
+    CK(cudaSetDevice(ctx->device));
+    char* scratch = nullptr;
+    int rc = noalloc_scratch(ctx, &scratch);
+    if (rc != NNLBM_OK) return rc;
+    // refuse everything that nnlbm_step would have to allocate, before any launch
+    for (size_t gi = 0; gi < ctx->groups.size(); ++gi) {
+        const Group& g = ctx->groups[gi];
+        if (g.dirty)
+            return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: launch group %zu has no device work list yet; call "
+                           "nnlbm_step or nnlbm_step_info once after the map is set", gi);
+        const size_t need = (size_t)g.n_self * 4 * (g.dtype == NNLBM_F64 ? 8 : 4);
+        if (need > NNLBM_NOALLOC_SCRATCH_BYTES - kNoallocHead)
+            return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: launch group %zu has %lld open-plane nodes written by "
+                           "their own thread, %zu bytes of scratch, above the %zu bytes of NNLBM_NOALLOC_SCRATCH_BYTES",
+                           gi, (long long)g.n_self, need, (size_t)NNLBM_NOALLOC_SCRATCH_BYTES - kNoallocHead);
+        int64_t parity = -1;
+        for (int ic : g.cases) {
+            const Case& c = ctx->cases[ic];
+            if (!c.has_map || !c.has_state) return set_err(ctx, NNLBM_ERR_ARG, "case %d has no map or initial state", ic);
+            if (parity >= 0 && c.parity != parity)
+                return set_err(ctx, NNLBM_ERR_ARG, "cases of one launch group are at different step parities "
+                               "(re-initialise or re-import all of them)");
+            parity = c.parity;
+            if (((flags & NNLBM_STEP_MACRO) || c.d.cy_mode == NNLBM_CY_REF_FD) && !c.d_macro)
+                return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: case %d has no macro buffer yet; run one "
+                               "nnlbm_step with NNLBM_STEP_MACRO first", ic);
+            if ((flags & NNLBM_STEP_STATS) && !c.d_stats)
+                return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: case %d has no mean/rms buffer yet; run one "
+                               "nnlbm_step with NNLBM_STEP_STATS first", ic);
+            if (n_steps > c.ctl_cap)
+                return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: %lld steps exceed the %lld control rows of case %d",
+                               (long long)n_steps, (long long)c.ctl_cap, ic);
+        }
+    }
+    int cursors[64];
+    int err = 0;
+    const size_t n_groups = ctx->groups.size();
+    if (n_groups > 64) return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: more than 64 launch groups");
+    for (size_t gi = 0; gi < n_groups; ++gi) {
+        Group& g = ctx->groups[gi];
+        const bool f64 = g.dtype == NNLBM_F64;
+        for (int ic : g.cases) {
+            Case& c = ctx->cases[ic];
+            rc = f64 ? upload_ctl_rows<double>(ctx, c, n_steps, flags) : upload_ctl_rows<float>(ctx, c, n_steps, flags);
+            if (rc != NNLBM_OK) return rc;
+            if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
+        }
+        // the two counters start at zero for every group; the group's steps, in stream
+        // order, finish before the next group clears them again
+        CK(cudaMemsetAsync(scratch, 0, 2 * sizeof(int), ctx->stream));
+        alignas(16) char args[sizeof(GroupArgs<double>)];
+        if (f64) noalloc_args<double>(g, scratch, args);
+        else noalloc_args<float>(g, scratch, args);
+        const AuxLaunchers& A = aux_launchers(g.dtype);
+        const int per_block = g.block / kChunk;
+        const dim3 cgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block), cblk(g.block);
+        const int64_t parity = ctx->cases[g.cases[0]].parity;
+        for (int64_t k = 0; k < n_steps; ++k) {
+            const bool odd = ((parity + k) & 1) != 0;
+            if (g.any_refd) {
+                A.refd_velocity(odd, cgrid, cblk, ctx->stream, args);
+                A.refd_stress(odd, cgrid, cblk, ctx->stream, args);
+            }
+            if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 127) / 128), dim3(128), ctx->stream, args);
+            step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, args);
+        }
+        CK(cudaGetLastError());
+        // pageable destination: the copy returns once the cursor is on the host
+        CK(cudaMemcpyAsync(&cursors[gi], scratch, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        finish_steps(ctx, g, n_steps, flags);
+    }
+    for (Case& c : ctx->cases) {
+        if (c.sched.empty()) continue;
+        const int64_t rows = (int64_t)c.sched.size() / 3;
+        if (n_steps < rows) c.sched.erase(c.sched.begin(), c.sched.begin() + 3 * n_steps);
+        else c.sched.erase(c.sched.begin(), c.sched.end() - 3);
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t gi = 0; gi < n_groups; ++gi)
+        if (cursors[gi] != n_steps)
+            return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", gi, cursors[gi],
+                           (long long)n_steps);
+    for (size_t i = 0; i < ctx->cases.size(); ++i) {
+        CK(cudaMemcpy(&err, ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
+    }
     return NNLBM_OK;
 }
 

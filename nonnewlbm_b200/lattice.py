@@ -119,6 +119,12 @@ class Lattice:
         flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0) | (capi.STEP_REDUCE if reduce else 0)
         self._chk(capi.lib().nnlbm_step(self.h, int(n), flags))
 
+    def step_noalloc(self, n: int = 1, stats: bool = False, macro: bool = False, reduce: bool = False) -> None:
+        """nnlbm_step_noalloc: the same steps without any device allocation (the buffers the
+        flags need must exist already; see include/nnlbm.h)."""
+        flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0) | (capi.STEP_REDUCE if reduce else 0)
+        self._chk(capi.lib().nnlbm_step_noalloc(self.h, int(n), flags))
+
     def autotune(self) -> None:
         self._chk(capi.lib().nnlbm_autotune(self.h))
 
