@@ -63,6 +63,11 @@ namespace {
 
 const int kStorageBytes[4] = {8, 4, 2, 2};
 const int kChunk = 32;
+// slack around the populations and after the labels: the staged rows of a chunk start at
+// the 16-byte boundary at or below the first element and end up to 16 bytes past the
+// chunk, which at the ends of the arrays reaches outside them
+const size_t kDfPad = 512;
+const size_t kLabelPad = 64;
 
 struct Case {
     nnlbm_case_desc d{};
@@ -71,6 +76,7 @@ struct Case {
     double scale = 1.0;      // 16-bit storage scale
     int group = 0;
     // device buffers
+    void* df_base = nullptr; // allocation holding df with kDfPad bytes on either side
     void* df = nullptr;      // 27 direction arrays
     size_t q_stride = 0;     // elements between direction arrays
     uint8_t* d_label = nullptr;
@@ -261,7 +267,7 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
         ca.push_back(*(const CaseArgs<CT>*)c.args.data());
         g.any_refd |= c.d.cy_mode == NNLBM_CY_REF_FD;
         for (int4 ch : c.chunks) {
-            ch.z = (int)j;
+            ch.z = (int)j | (ch.z & ~CH_CASE_MASK);
             ch.w += (int)self_off;
             chunks.push_back(ch);
         }
@@ -412,8 +418,10 @@ int wait_and_check(nnlbm_ctx* ctx, int64_t n)
     for (size_t i = 0; i < ctx->groups.size(); ++i)
         if (cur[2 * i] != n)
             return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", i, cur[2 * i], (long long)n);
-    for (size_t i = 0; i < ctx->cases.size(); ++i)
+    for (size_t i = 0; i < ctx->cases.size(); ++i) {
+        if (err[i] & 2) return set_err(ctx, NNLBM_ERR_TIMEOUT, "case %zu: a staged chunk did not arrive in time", i);
         if (err[i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
+    }
     return NNLBM_OK;
 }
 
@@ -538,7 +546,7 @@ extern "C" {
 
 int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx** out)
 {
-    if (!desc || n_cases < 1 || !out) return NNLBM_ERR_ARG;
+    if (!desc || n_cases < 1 || n_cases > CH_CASE_MASK + 1 || !out) return NNLBM_ERR_ARG;
     nnlbm_ctx* ctx = new nnlbm_ctx();
     *out = ctx; // on failure the context carries the message; the caller destroys it
     ctx->device = device;
@@ -568,11 +576,13 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
                   : (d.dtype == NNLBM_F16 ? 1024.0 : 1.0);
         const size_t eb = kStorageBytes[d.dtype];
         c.q_stride = ((size_t)c.N + 127) / 128 * 128;
-        if (cudaMalloc(&c.df, 27 * c.q_stride * eb) != cudaSuccess || cudaMalloc(&c.d_label, (size_t)c.N) != cudaSuccess ||
+        if (cudaMalloc(&c.df_base, 27 * c.q_stride * eb + 2 * kDfPad) != cudaSuccess ||
+            cudaMalloc(&c.d_label, ((size_t)c.N + kLabelPad + 15) / 16 * 16) != cudaSuccess ||
             cudaMalloc(&c.d_red, 8 * sizeof(double)) != cudaSuccess || cudaMalloc(&c.d_err, sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
             return set_err(ctx, NNLBM_ERR_OOM, "case %d: device allocation of %.2f GB failed", i, 27.0 * c.q_stride * eb / 1e9);
         }
+        c.df = (char*)c.df_base + kDfPad;
         cudaMemset(c.d_red, 0, 8 * sizeof(double));
         cudaMemset(c.d_err, 0, sizeof(int));
         c.label.assign((size_t)c.N, (uint8_t)L_WALL);
@@ -657,25 +667,32 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                     dl[i] |= LF_SELF;
                 }
             }
-    // packed work list of 32-cell row chunks and the self-handled nodes
+    // packed work list of 32-cell row chunks and the self-handled nodes: a chunk starts at
+    // the first cell with work not yet covered in its row, so a short row segment fills
+    // one chunk instead of straddling two
     std::vector<int4> chunks;
     std::vector<int32_t> self_cell, gather_self;
+    auto has_work = [&](size_t i) { return map[i] == L_FLUID || map[i] == L_PERIODIC || (dl[i] & LF_SELF); };
     for (int z = 0; z < nz; ++z)
         for (int y = 0; y < ny; ++y)
             for (int x0 = 0; x0 < nx; x0 += kChunk) {
+                while (x0 < nx && !has_work(id(x0, y, z))) ++x0;
+                if (x0 >= nx) break;
                 const int self_base = (int)self_cell.size();
-                bool work = false;
+                bool work = false, fluid = false;
                 for (int x = x0; x < std::min(nx, x0 + kChunk); ++x) {
                     const size_t i = id(x, y, z);
                     const int lab = map[i];
-                    if (lab == L_FLUID || lab == L_PERIODIC) work = true;
+                    if (lab == L_FLUID || lab == L_PERIODIC) work = fluid = true;
                     if (dl[i] & LF_SELF) {
                         work = true;
                         if (lab != L_IN_EQ) gather_self.push_back((int32_t)self_cell.size());
                         self_cell.push_back((int32_t)i);
                     }
                 }
-                if (work) chunks.push_back(make_int4((int)id(x0, y, z), y | (z << 16), 0, self_base));
+                // flags: the chunk has colliding cells; the chunk lies on a y or z face
+                const int fl = (fluid ? CH_FLUID : 0) | (y == 0 || y == ny - 1 || z == 0 || z == nz - 1 ? CH_FACE : 0);
+                if (work) chunks.push_back(make_int4((int)id(x0, y, z), y | (z << 16), fl, self_base));
             }
     c.label.assign(map, map + c.N);
     c.dlabel = dl;
@@ -1185,6 +1202,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
                            (long long)n_steps);
     for (size_t i = 0; i < ctx->cases.size(); ++i) {
         CK(cudaMemcpy(&err, ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err & 2) return set_err(ctx, NNLBM_ERR_TIMEOUT, "case %zu: a staged chunk did not arrive in time", i);
         if (err) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
     }
     return NNLBM_OK;
@@ -1215,7 +1233,7 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
             if (p) cudaFree(p);
     }
     for (Case& c : ctx->cases) {
-        void* ptrs[] = {c.df, c.d_label, c.d_macro, c.d_stats, c.d_ctl, c.d_red, c.d_err};
+        void* ptrs[] = {c.df_base, c.d_label, c.d_macro, c.d_stats, c.d_ctl, c.d_red, c.d_err};
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }

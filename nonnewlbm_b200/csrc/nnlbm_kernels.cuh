@@ -33,6 +33,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <atomic>
+
 #include "nnlbm_physics.cuh"
 
 namespace nnlbm {
@@ -53,22 +56,26 @@ enum : int { M_RHO = 0, M_VX, M_VY, M_VZ, M_FX, M_FY, M_FZ, M_S11, M_S12, M_S13,
 template <int DT> struct Storage;
 template <> struct Storage<0> {
     using T = double; using CT = double;
+    __device__ static __forceinline__ CT from(T v, int, CT) { return v; }
     __device__ static __forceinline__ CT load(const T* p, int i, int, CT) { return p[i]; }
     __device__ static __forceinline__ void store(T* p, int i, int, CT v, CT) { p[i] = v; }
 };
 template <> struct Storage<1> {
     using T = float; using CT = float;
+    __device__ static __forceinline__ CT from(T v, int q, CT) { return weight<float>(q) + v; }
     __device__ static __forceinline__ CT load(const T* p, int i, int q, CT) { return weight<float>(q) + p[i]; }
     __device__ static __forceinline__ void store(T* p, int i, int q, CT v, CT) { p[i] = v - weight<float>(q); }
 };
 template <> struct Storage<2> {
     using T = __half; using CT = float;
-    __device__ static __forceinline__ CT load(const T* p, int i, int q, CT isc) { return weight<float>(q) + __half2float(p[i]) * isc; }
+    __device__ static __forceinline__ CT from(T v, int q, CT isc) { return weight<float>(q) + __half2float(v) * isc; }
+    __device__ static __forceinline__ CT load(const T* p, int i, int q, CT isc) { return from(p[i], q, isc); }
     __device__ static __forceinline__ void store(T* p, int i, int q, CT v, CT sc) { p[i] = __float2half_rn((v - weight<float>(q)) * sc); }
 };
 template <> struct Storage<3> {
     using T = __nv_bfloat16; using CT = float;
-    __device__ static __forceinline__ CT load(const T* p, int i, int q, CT isc) { return weight<float>(q) + __bfloat162float(p[i]) * isc; }
+    __device__ static __forceinline__ CT from(T v, int q, CT isc) { return weight<float>(q) + __bfloat162float(v) * isc; }
+    __device__ static __forceinline__ CT load(const T* p, int i, int q, CT isc) { return from(p[i], q, isc); }
     __device__ static __forceinline__ void store(T* p, int i, int q, CT v, CT sc) { p[i] = __float2bfloat16_rn((v - weight<float>(q)) * sc); }
 };
 
@@ -139,15 +146,18 @@ __device__ __forceinline__ void accumulate_stats(const CaseArgs<CT>& a, int c, C
     // MacroTcpc::outputMacro (sim_tcpc.cu:347-353); the sign split of rho*ux is summed
     const CT jx = rho * ux, jy = rho * uy, jz = rho * uz;
     const int64_t N = a.N;
+    // one contribution per cell and step: fire-and-forget reductions in L2 give the same
+    // sums as a read-modify-write without exposing the read latency
     if (a.stats_f64) {
         double* s = (double*)a.stats;
-        s[c] += (double)jx; s[N + c] += (double)jy; s[2 * N + c] += (double)jz;
-        s[3 * N + c] += (double)jx * (double)jx; s[4 * N + c] += (double)jy * (double)jy;
-        s[5 * N + c] += (double)jz * (double)jz;
+        atomicAdd(s + c, (double)jx); atomicAdd(s + N + c, (double)jy); atomicAdd(s + 2 * N + c, (double)jz);
+        atomicAdd(s + 3 * N + c, (double)jx * (double)jx); atomicAdd(s + 4 * N + c, (double)jy * (double)jy);
+        atomicAdd(s + 5 * N + c, (double)jz * (double)jz);
     } else {
         float* s = (float*)a.stats;
-        s[c] += (float)jx; s[N + c] += (float)jy; s[2 * N + c] += (float)jz;
-        s[3 * N + c] += (float)(jx * jx); s[4 * N + c] += (float)(jy * jy); s[5 * N + c] += (float)(jz * jz);
+        atomicAdd(s + c, (float)jx); atomicAdd(s + N + c, (float)jy); atomicAdd(s + 2 * N + c, (float)jz);
+        atomicAdd(s + 3 * N + c, (float)(jx * jx)); atomicAdd(s + 4 * N + c, (float)(jy * jy));
+        atomicAdd(s + 5 * N + c, (float)(jz * jz));
     }
 }
 
@@ -255,7 +265,7 @@ __device__ __noinline__ void refd_force(const CaseArgs<CT>& a, int c, int sy, in
 // minimum resident blocks of 256 threads: the register budget of each variant (FP64
 // arithmetic and the KBC family need more live values than the cumulant in FP32)
 #ifndef NNLBM_STEP_MINB
-#define NNLBM_STEP_MINB 3
+#define NNLBM_STEP_MINB 2
 #endif
 template <int DT, int COL>
 struct StepOccupancy {
@@ -263,49 +273,164 @@ struct StepOccupancy {
 };
 
 // ---------------------------------------------------------------------------------------
-// the fused step (solver/lbm3d/core.h:578-800): FLUID / PERIODIC cells collide, source
-// cells also finish their fused open-plane neighbours, self-handled nodes write their
-// equilibrium
+// shared-memory staging of a chunk with TMA bulk copies (cp.async.bulk global -> shared,
+// completion counted in bytes on an mbarrier); no cluster, no multicast
+// ---------------------------------------------------------------------------------------
+// chunk record flags (bits 16.. of the case word)
+enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// one bounded probe of the phase; the hint caps the suspension at 20 microseconds
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity), "r"(20000u)
+                 : "memory");
+    return done != 0;
+}
+
+// wait for a phase with an iteration limit (about two seconds); false when it ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (int it = 0; it < 100000; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// `bytes` (a multiple of 16) from 16-byte aligned global memory into shared memory
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// one pipeline stage of a warp: the 27 population rows of its chunk, each copied from the
+// 16-byte boundary at or below the row's first element (so a row spans 32 elements plus
+// up to 16 bytes of slack), and the chunk's label row likewise
+template <int DT>
+struct Stage {
+    static constexpr int S = (int)sizeof(typename Storage<DT>::T);
+    static constexpr int RB = 32 * S + 16;
+    static constexpr int LB = 48;
+    static constexpr int BYTES = 27 * RB + LB;
+};
+// per warp: two mbarriers (16 B) and a ring of its next 32 chunk records (512 B), then
+// the two stages; up to 8 warps per block
+constexpr int kRing = 32;
+constexpr int kStepSmemHead = 8 * (16 + kRing * 16);
+template <int DT>
+constexpr int step_smem_bytes(int warps_per_block) { return kStepSmemHead + warps_per_block * 2 * Stage<DT>::BYTES; }
+
+// start the copies of chunk `rec` into stage `stg`; returns the bytes the stage's
+// mbarrier expects (0: the chunk loads directly from global memory)
+template <int DT, bool ODD, bool SINGLE>
+__device__ __forceinline__ uint32_t issue_chunk(const GroupArgs<typename Storage<DT>::CT>& g, int4 rec, unsigned char* stg,
+                                                uint32_t bar, int lane)
+{
+    using G = Stage<DT>;
+    using CT = typename Storage<DT>::CT;
+    // an odd step of a chunk on a y/z face pulls across the face (wrapped rows)
+    if (ODD && (rec.z & CH_FACE)) return 0;
+    const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[rec.z & CH_CASE_MASK];
+    const bool fluid = (rec.z & CH_FLUID) != 0;
+    const uint32_t bytes = fluid ? (uint32_t)(27 * G::RB + G::LB) : (uint32_t)G::LB;
+    if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
+    __syncwarp();
+    const int c0 = rec.x;
+    if (lane < 27) {
+        if (fluid) {
+            const int q = lane;
+            // even: slot q at the chunk's cells; odd: slot opp(q) at the cells - c_q
+            const int slot = ODD ? oppq(q) : q;
+            const int cs = ODD ? c0 - (cxq(q) + a.nx * cyq(q) + a.nx * a.ny * czq(q)) : c0;
+            const int64_t off = ((int64_t)slot * a.qstride + cs) * G::S;
+            bulk_g2s(smem_u32(stg) + q * G::RB, (const char*)a.df + (off & ~(int64_t)15), G::RB, bar);
+        }
+    } else if (lane == 27) {
+        bulk_g2s(smem_u32(stg) + 27 * G::RB, a.label + (c0 & ~15), G::LB, bar);
+    }
+    return bytes;
+}
+
+// ---------------------------------------------------------------------------------------
+// one 32-cell chunk of the fused step (solver/lbm3d/core.h:578-800): FLUID / PERIODIC
+// cells collide, source cells also finish their fused open-plane neighbours,
+// self-handled nodes write their equilibrium.  `stg` is the chunk's staged rows, or null
+// when the chunk loads directly from global memory.
 // ---------------------------------------------------------------------------------------
 template <int DT, int COL, bool ODD, bool SINGLE>
-__global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
-    k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
+__device__ __forceinline__ void process_chunk(const GroupArgs<typename Storage<DT>::CT>& g, int4 ch, const unsigned char* stg,
+                                              int step, int lane)
 {
     using S = Storage<DT>;
+    using T = typename S::T;
     using CT = typename S::CT;
-    const int lane = threadIdx.x & 31;
-    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-    const bool valid = warp < g.n_chunks;
-    const int4 ch = valid ? g.chunks[warp] : make_int4(0, 0, 0, 0);
-    // a single-case group reads its parameters from the constant bank
-    const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[ch.z];
-    const int step = *g.cursor;
+    using G = Stage<DT>;
+    const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[ch.z & CH_CASE_MASK];
     const int y = ch.y & 0xffff, z = ch.y >> 16;
     const int sy = a.nx, sz = a.nx * a.ny;
     const int x0 = ch.x - y * sy - z * sz;
     const int x = x0 + lane;
-    const bool inb = valid && x < a.nx;
+    const bool inb = x < a.nx;
     const int c = ch.x + lane;
-    const int raw = inb ? (int)a.label[c] : L_WALL;
+    const int raw = !inb ? (int)L_WALL : stg ? (int)stg[27 * G::RB + (ch.x & 15) + lane] : (int)a.label[c];
     const int lab = raw & L_MASK;
     const bool fluid = lab == L_FLUID || lab == L_PERIODIC;
     const bool self = (raw & LF_SELF) != 0;
     const unsigned selfmask = __ballot_sync(0xffffffffu, self);
-    const int flags = valid ? a.ctl[step].flags : 0;
+    const int flags = a.ctl[step].flags;
     double mass = 0.0, q3 = 0.0, q4 = 0.0, q5 = 0.0, q6 = 0.0;
     if (fluid) {
-        const bool interior = x > 0 && x < a.nx - 1 && y > 0 && y < a.ny - 1 && z > 0 && z < a.nz - 1;
+        const bool xin = x > 0 && x < a.nx - 1;
+        // odd steps: index corrections of the wrapped neighbours (zero inside the box);
+        // w*m apply to a neighbour at coordinate - 1, w*p to one at coordinate + 1
+        const int wxm = x == 0 ? a.nx : 0, wxp = x == a.nx - 1 ? -a.nx : 0;
+        const int wym = y == 0 ? sz : 0, wyp = y == a.ny - 1 ? -sz : 0;
+        const int wzm = z == 0 ? (int)a.N : 0, wzp = z == a.nz - 1 ? -(int)a.N : 0;
+        auto nbr = [&](int q, int sign) -> int { // cell at x + sign c_q
+            const int dx = sign * cxq(q), dy = sign * cyq(q), dz = sign * czq(q);
+            return c + dx + sy * dy + sz * dz + (dx < 0 ? wxm : dx > 0 ? wxp : 0) + (dy < 0 ? wym : dy > 0 ? wyp : 0) +
+                   (dz < 0 ? wzm : dz > 0 ? wzp : 0);
+        };
         CT f[27];
         if (!ODD) {
+            // even steps always have the chunk staged: the element of this lane sits
+            // (first element mod 16) bytes into its row, plus lane * element size
+            const unsigned char* p = stg + lane * G::S + (((unsigned)ch.x * (unsigned)G::S) & 15u);
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = S::load(qptr<DT>(a, q), c, q, a.inv_scale);
-        } else {
+            for (int q = 0; q < 27; ++q) f[q] = S::from(*(const T*)(p + q * G::RB), q, a.inv_scale);
+        } else if (stg && xin) {
+            const unsigned char* p = stg + lane * G::S;
+            const unsigned c0b = (unsigned)ch.x * (unsigned)G::S;
+            const unsigned syb = (unsigned)sy * (unsigned)G::S, szb = (unsigned)sz * (unsigned)G::S;
 #pragma unroll
             for (int q = 0; q < 27; ++q) {
-                const int nb = interior ? c - (cxq(q) + sy * cyq(q) + sz * czq(q))
-                                        : wrapc(x - cxq(q), a.nx) + sy * wrapc(y - cyq(q), a.ny) + sz * wrapc(z - czq(q), a.nz);
-                f[q] = S::load(qptr<DT>(a, oppq(q)), nb, q, a.inv_scale);
+                const unsigned d = (c0b - (unsigned)(cxq(q) * G::S) - (unsigned)cyq(q) * syb - (unsigned)czq(q) * szb) & 15u;
+                f[q] = S::from(*(const T*)(p + q * G::RB + d), q, a.inv_scale);
             }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 27; ++q) f[q] = S::load(qptr<DT>(a, oppq(q)), nbr(q, -1), q, a.inv_scale);
         }
         CT fx = a.fx, fy = a.fy, fz = a.fz;
         if (a.cy_mode == CY_REF_FD && lab == L_FLUID) {
@@ -343,23 +468,22 @@ __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
                 else if (nl == L_OUT_B) q6 += qn;
             }
         }
+        // one inlined collision for both viscosity models (the local Carreau-Yasuda law is
+        // a runtime branch inside it)
         CT Sl[6];
-        if (a.cy_mode == CY_LOCAL_NEQ) {
-            const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
-            collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu, &cy, Sl);
-        } else {
-            collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu);
-        }
+        const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
+        collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
+        // one running pointer over the direction arrays keeps the 27 store addresses out
+        // of the register file
+        const int64_t qs = a.qstride;
         if (!ODD) {
+            T* p = (T*)a.df + (c + 26 * qs);
 #pragma unroll
-            for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, oppq(q)), c, q, f[q], a.scale);
+            for (int q = 0; q < 27; ++q, p -= qs) S::store(p, 0, q, f[q], a.scale);
         } else {
+            T* p = (T*)a.df;
 #pragma unroll
-            for (int q = 0; q < 27; ++q) {
-                const int nb = interior ? c + (cxq(q) + sy * cyq(q) + sz * czq(q))
-                                        : wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz);
-                S::store(qptr<DT>(a, q), nb, q, f[q], a.scale);
-            }
+            for (int q = 0; q < 27; ++q, p += qs) S::store(p, nbr(q, 1), q, f[q], a.scale);
         }
         if ((flags & F_MACRO) || a.cy_mode == CY_REF_FD) {
             write_macro<CT>(a, c, rho, ux, uy, uz, fx, fy, fz);
@@ -399,6 +523,72 @@ __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
             if (s3 != 0.0) atomicAdd(a.red + 3, s3);
             if (s4 != 0.0) atomicAdd(a.red + 4, s4);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// the step kernel: persistent warps walk the chunk list with a stride of all warps of the
+// grid; each warp stages its next chunk in shared memory (two stages) while it computes
+// the current one.  The last block to finish advances the step cursor.
+// ---------------------------------------------------------------------------------------
+template <int DT, int COL, bool ODD, bool SINGLE>
+__global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
+    k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
+{
+    using G = Stage<DT>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const uint32_t bar0 = smem_u32(smem) + 16 * wib;
+    int4* const ring = (int4*)(smem + 8 * 16) + wib * kRing;
+    unsigned char* const stg0 = smem + kStepSmemHead + wib * 2 * G::BYTES;
+    if (lane == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        fence_mbar_init();
+    }
+    const int n = g.n_chunks;
+    const int W = (int)gridDim.x * wpb;
+    const int step = *g.cursor;
+    const int i0 = (int)blockIdx.x * wpb + wib;
+    // the records of this warp's chunks k = 0..31 (chunk i0 + k W), refilled every 32
+    {
+        const int i = i0 + lane * W;
+        if (i < n) ring[lane] = g.chunks[i];
+    }
+    __syncwarp();
+    uint32_t bytes_cur = i0 < n ? issue_chunk<DT, ODD, SINGLE>(g, ring[0], stg0, bar0, lane) : 0u, bytes_nxt = 0;
+    uint32_t parity = 0; // bit s: phase parity of stage s
+    int s = 0, k = 0;
+    bool ok = true;
+    for (int i = i0; i < n; i += W, ++k, s ^= 1) {
+        const int4 cur = ring[k & (kRing - 1)];
+        if (((k + 1) & (kRing - 1)) == 0) {
+            // refill the ring with the records of chunks k+1 .. k+32
+            __syncwarp();
+            const int j = i + (lane + 1) * W;
+            if (j < n) ring[lane] = g.chunks[j];
+            __syncwarp();
+        }
+        // stage the next chunk while this one computes
+        bytes_nxt = i + W < n ? issue_chunk<DT, ODD, SINGLE>(g, ring[(k + 1) & (kRing - 1)], stg0 + (s ^ 1) * G::BYTES,
+                                                             bar0 + 8 * (s ^ 1), lane)
+                              : 0u;
+        if (bytes_cur) {
+            ok = __all_sync(0xffffffffu, mbar_wait(bar0 + 8 * s, (parity >> s) & 1u));
+            if (!ok) {
+                // a staged chunk never arrived: flag it, let the copies in flight land, stop
+                if (lane == 0) atomicOr(SINGLE ? g.c0.err : g.cases[cur.z & CH_CASE_MASK].err, 2);
+                mbar_wait(bar0 + 8 * s, (parity >> s) & 1u);
+                if (bytes_nxt) mbar_wait(bar0 + 8 * (s ^ 1), (parity >> (s ^ 1)) & 1u);
+                break;
+            }
+            parity ^= 1u << s;
+        }
+        process_chunk<DT, COL, ODD, SINGLE>(g, cur, bytes_cur ? stg0 + s * G::BYTES : nullptr, step, lane);
+        // all reads of this stage are done before the next copy into it
+        fence_proxy_async_smem();
+        __syncwarp();
+        bytes_cur = bytes_nxt;
     }
     // the last block to finish advances the step cursor (every block has read it above)
     __syncthreads();
@@ -499,7 +689,7 @@ __global__ void __launch_bounds__(256) k_refd_velocity(const __grid_constant__ G
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (warp >= g.n_chunks) return;
     const int4 ch = g.chunks[warp];
-    const CaseArgs<CT>& a = g.cases[ch.z];
+    const CaseArgs<CT>& a = g.cases[ch.z & CH_CASE_MASK];
     if (a.cy_mode != CY_REF_FD) return;
     const int y = ch.y & 0xffff, z = ch.y >> 16;
     const int x = ch.x - y * a.nx - z * a.nx * a.ny + lane;
@@ -522,7 +712,7 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (warp >= g.n_chunks) return;
     const int4 ch = g.chunks[warp];
-    const CaseArgs<CT>& a = g.cases[ch.z];
+    const CaseArgs<CT>& a = g.cases[ch.z & CH_CASE_MASK];
     if (a.cy_mode != CY_REF_FD) return;
     const int sy = a.nx, sz = a.nx * a.ny;
     const int y = ch.y & 0xffff, z = ch.y >> 16;
@@ -557,17 +747,48 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
 // ---------------------------------------------------------------------------------------
 using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 
+// launch of one step-kernel variant: the dynamic shared memory is opted in once per
+// device, and the grid is capped at the blocks that are resident at once (persistent)
+template <int DT, int COL, bool ODD, bool SINGLE>
+void launch_step_variant(dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
+{
+    auto kern = k_step<DT, COL, ODD, SINGLE>;
+    const int smem = step_smem_bytes<DT>((int)block.x / 32);
+    static std::atomic<unsigned long long> attr_set{0};
+    static std::atomic<int> resident[9] = {};  // per block size / 32
+    static std::atomic<int> sm_count{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load() & bit)) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, step_smem_bytes<DT>(8));
+        attr_set.fetch_or(bit);
+    }
+    const int wpb = (int)block.x / 32;
+    if (wpb < 1 || wpb > 8) return;
+    if (!resident[wpb].load()) {
+        int nb = 0, sms = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, (int)block.x, smem);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        sm_count.store(std::max(sms, 1));
+        resident[wpb].store(std::max(nb, 1));
+    }
+    const unsigned cap = (unsigned)(resident[wpb].load() * sm_count.load());
+    const dim3 gr(std::max(1u, std::min(grid.x, cap)));
+    kern<<<gr, block, smem, s>>>(g);
+}
+
 template <int DT, int COL>
 void launch_step(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
     if (g.n_cases == 1) {
-        if (odd) k_step<DT, COL, true, true><<<grid, block, 0, s>>>(g);
-        else k_step<DT, COL, false, true><<<grid, block, 0, s>>>(g);
+        if (odd) launch_step_variant<DT, COL, true, true>(grid, block, s, g);
+        else launch_step_variant<DT, COL, false, true>(grid, block, s, g);
     } else {
-        if (odd) k_step<DT, COL, true, false><<<grid, block, 0, s>>>(g);
-        else k_step<DT, COL, false, false><<<grid, block, 0, s>>>(g);
+        if (odd) launch_step_variant<DT, COL, true, false>(grid, block, s, g);
+        else launch_step_variant<DT, COL, false, false>(grid, block, s, g);
     }
 }
 
