@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--dtype", default="f32")
     ap.add_argument("--collision", default="CUM")
     ap.add_argument("--cy-mode", default="local-neq")
+    ap.add_argument("--workload", default="junction", choices=["junction", "dense_box"])
+    ap.add_argument("--shape", default=None, help="dense box nx,ny,nz (default 768,576,480)")
     ap.add_argument("--no-stats", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=400)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -157,35 +159,66 @@ def bytes_per_update(dtype: str, stats: bool, stats_f64: bool = True) -> float:
     return float(b)
 
 
+def workload(a, dtype=None):
+    """The measured case: the junction configuration (sparse TCPC junction with
+    Carreau-Yasuda blood) or the dense-box throughput configuration."""
+    from nonnewlbm_b200 import workloads as W
+
+    dt = dtype or a.dtype
+    if a.workload == "dense_box":
+        shape = tuple(int(v) for v in a.shape.split(",")) if a.shape else (768, 576, 480)
+        return W.dense_box(dtype=dt, collision=a.collision, shape=shape)
+    return W.junction_cy(dtype=dt, collision=a.collision, cy_mode=a.cy_mode)
+
+
+def reference_lattice(w, collision: str):
+    """The reference's own headers (oracle/_ref, single precision like the production
+    build) on the workload's lattice; the dense box is sampled as an 8-cell slab in z.
+    Returns (RefLattice, fluid cells, sample text)."""
+    import oracle as O
+    from nonnewlbm_b200 import geometry as G
+
+    nx, ny, nz = w.shape
+    if w.kind == "tcpc":
+        orc = O.Oracle(nx, ny, nz)
+        rc, counts = orc.setup_tcpc(w.wall)
+        m = orc.get_map()
+        del orc
+        ref = O.RefLattice(nx, ny, nz, collision=O.COLLISIONS.index(collision), equilibrium=O.EQ_INV_CUM_REF,
+                           nu=w.nu, prec=4, fast=True)
+        ref.set_map(m)
+        ref.set_inflow(ivc_flux=w.u_ivc * counts[0], svc_flux=w.u_svc * counts[1])
+        what = (f"the full {nx}x{ny}x{nz} junction; the single-rank reference leaves Carreau-Yasuda inert "
+                f"(zero strain), so the Newtonian step is timed")
+    else:
+        nz = min(nz, 8)
+        m, prof = G.dense_box_map(nx, ny, nz)
+        ref = O.RefLattice(nx, ny, nz, collision=O.COLLISIONS.index(collision), equilibrium=O.EQ_INV_CUM_REF,
+                           nu=w.nu, prec=4, fast=True)
+        ref.set_map(m)
+        ref.set_inflow_profile(G.expand_profile(m, prof) * w.u_ivc)
+        what = f"a {nx}x{ny}x{nz} slab of the dense box (same rows, periodic in y and z)"
+    ref.init_equilibrium()
+    fluid = int(np.count_nonzero((m == G.MAP_FLUID) | (m == G.MAP_PERIODIC)))
+    return ref, fluid, what
+
+
 def run_reference(a, dist: Dist):
-    """The reference's own collision/streaming headers (oracle/_ref, single precision like
-    the production build) driven by the single-rank host loop, on the same lattice."""
+    """Times the reference's own per-cell collision / streaming headers on the host cores."""
     if dist.rank != 0:
         return 0
     import oracle as O
-    from nonnewlbm_b200 import geometry as G
-    from nonnewlbm_b200 import workloads as W
 
     if not O.ref_available(fast=True):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnnlbm_ref_fast.so not built "
                           "(the reference checkout was absent at build time)"}))
         return 0
-    w = W.junction_cy(dtype="f32", collision=a.collision)
-    nx, ny, nz = w.shape
-    lib = O.ref_lib(fast=True)
+    w = workload(a, "f32")
     threads = os.cpu_count() or 1
-    lib.ref_set_threads(threads)
-    orc = O.Oracle(nx, ny, nz)
-    rc, counts = orc.setup_tcpc(w.wall)
-    m = orc.get_map()
-    del orc
-    ref = O.RefLattice(nx, ny, nz, collision=O.COLLISIONS.index(a.collision), equilibrium=O.EQ_INV_CUM_REF, nu=w.nu,
-                       prec=4, fast=True)
-    ref.set_map(m)
-    ref.set_inflow(ivc_flux=w.u_ivc * counts[0], svc_flux=w.u_svc * counts[1])
-    ref.init_equilibrium()
-    fluid = int(np.count_nonzero((m == G.MAP_FLUID) | (m == G.MAP_PERIODIC)))
-    for _ in range(max(1, min(a.warmup, 2))):
+    O.ref_lib(fast=True).ref_set_threads(threads)
+    ref, fluid, what = reference_lattice(w, a.collision)
+    warm = max(1, min(a.warmup, 2))
+    for _ in range(warm):
         ref.step(1, accumulate_stats=not a.no_stats)
     times = []
     t_end = time.perf_counter() + a.cpu_seconds
@@ -197,14 +230,13 @@ def run_reference(a, dist: Dist):
         steps += 1
     sec = float(np.mean(times))
     mlups = fluid / sec / 1e6
-    sample = (f"{steps} steps of the full {nx}x{ny}x{nz} junction (fluid {fluid} cells) on {threads} host threads, "
-              f"reference cumulant + streaming headers in single precision (TraitsSP); the single-rank reference "
-              f"leaves Carreau-Yasuda inert (zero strain), so the Newtonian step is timed")
+    sample = (f"{steps} steps of {what} ({fluid} fluid cells) on {threads} host threads, reference collision and "
+              f"streaming headers in single precision (TraitsSP)")
     line = {"impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": a.gpus,
-            "steps": steps, "warmup": max(1, min(a.warmup, 2)), "ms_per_step": round(sec * 1e3, 3),
+            "steps": steps, "warmup": warm, "ms_per_step": round(sec * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": w.name, "collision": a.collision, "storage": "f32 (reference TraitsSP)",
-                       "cells": nx * ny * nz, "fluid_cells": fluid},
+                       "cells": int(np.prod(w.shape)), "fluid_cells_timed": fluid},
             "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -214,24 +246,13 @@ def run_reference(a, dist: Dist):
 
 def cpu_baseline_sample(w, seconds: float, collision: str) -> dict:
     import oracle as O
-    from nonnewlbm_b200 import geometry as G
 
     if not O.ref_available(fast=True):
         return {"value": None, "unit": "MLUPS", "cores": 0, "kind": "reference", "sample": "oracle/_ref not built"}
-    nx, ny, nz = w.shape
-    lib = O.ref_lib(fast=True)
     threads = os.cpu_count() or 1
-    lib.ref_set_threads(threads)
-    orc = O.Oracle(nx, ny, nz)
-    rc, counts = orc.setup_tcpc(w.wall)
-    m = orc.get_map()
-    del orc
-    ref = O.RefLattice(nx, ny, nz, collision=O.COLLISIONS.index(collision), nu=w.nu, prec=4, fast=True)
-    ref.set_map(m)
-    ref.set_inflow(ivc_flux=w.u_ivc * counts[0], svc_flux=w.u_svc * counts[1])
-    ref.init_equilibrium()
+    O.ref_lib(fast=True).ref_set_threads(threads)
+    ref, fluid, what = reference_lattice(w, collision)
     ref.step(1)
-    fluid = int(np.count_nonzero((m == G.MAP_FLUID) | (m == G.MAP_PERIODIC)))
     t0 = time.perf_counter()
     n = 0
     while n < 2 or time.perf_counter() - t0 < seconds:
@@ -239,8 +260,8 @@ def cpu_baseline_sample(w, seconds: float, collision: str) -> dict:
         n += 1
     sec = (time.perf_counter() - t0) / n
     return {"value": round(fluid / sec / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": "reference",
-            "sample": f"{n} steps of the same junction ({fluid} fluid cells), reference headers in single precision, "
-                      f"{threads} OpenMP threads; Carreau-Yasuda inert as in the single-rank reference"}
+            "sample": f"{n} steps of {what} ({fluid} fluid cells), reference headers in single precision, "
+                      f"{threads} OpenMP threads"}
 
 
 def main() -> int:
@@ -264,7 +285,7 @@ def run_ours(a, dist: Dist) -> int:
     dev = dist.local
     torch.cuda.set_device(dev)
     stats = not a.no_stats
-    w = W.junction_cy(dtype=a.dtype, collision=a.collision, cy_mode=a.cy_mode)
+    w = workload(a)
     lat = W.build_lattice(w, device=dev)
     info = lat.step_info()
     lat.autotune()
@@ -305,12 +326,15 @@ def run_ours(a, dist: Dist) -> int:
     bpu = bytes_per_update(a.dtype, stats)
     peak, peak_kind = measured_peaks()
     achieved = fluid * bpu / (t_step_ms / 1e3) / 1e9
-    key = f"{w.name}:{a.dtype}:{a.collision}:{a.cy_mode}:{'stats' if stats else 'nostats'}"
+    key = f"{w.name}:{a.dtype}:{a.collision}:{w.cy_mode}:{'stats' if stats else 'nostats'}"
     traffic = ncu_traffic(key)
 
     # end to end through the public API: per step the host sends that step's inflow row
     # (pinned staging inside the library) and reads back the FP64 mass / flux sums
-    rows = np.array([[w.u_ivc * w.notes["counts"]["left_area"], w.u_svc * w.notes["counts"]["right_area"], 1.0]])
+    if w.kind == "tcpc":
+        rows = np.array([[w.u_ivc * w.notes["counts"]["left_area"], w.u_svc * w.notes["counts"]["right_area"], 1.0]])
+    else:
+        rows = np.array([[0.0, 0.0, 1.0]])
     dist.barrier()
     t0 = time.perf_counter()
     red = None
@@ -332,7 +356,7 @@ def run_ours(a, dist: Dist) -> int:
             "scaling": "weak", "vs_baseline": None, "dtype": a.dtype, "data": "synthetic",
             "config": {"workload": w.name, "timing": "per-step CUDA events; before every step L2 is flushed by a 512 MB "
                                                       "write followed by a 256 MB read (clean lines)", "shape": list(w.shape), "fluid_cells": fluid, "collision": a.collision,
-                       "cy_mode": a.cy_mode, "storage": a.dtype, "stats": "fp64 mean/rms" if stats else "off",
+                       "cy_mode": w.cy_mode, "storage": a.dtype, "stats": "fp64 mean/rms" if stats else "off",
                        "bc_cells": info["bc_cells"], "parallelism": f"replicas x{dist.world}",
                        "dt_s": w.notes.get("dt_s"), "dx_m": w.notes.get("dx_m")},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",

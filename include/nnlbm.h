@@ -154,7 +154,7 @@ int nnlbm_set_schedule(nnlbm_ctx* ctx, int ic, const double* rows, int64_t n);
 int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags);
 
 /* Size of the one scratch array that nnlbm_step_noalloc uses on each device: two step
- * counters (256 bytes) plus, per launch group, four values (rho, ux, uy, uz) of the
+ * cursors (256 bytes) plus, per launch group, four values (rho, ux, uy, uz) of the
  * arithmetic type for each open-plane node that its own thread writes (nnlbm_step_info's
  * bc_cells bounds that count).  4 MiB holds 262,128 such nodes in FP32 arithmetic and
  * 131,064 in FP64. */
@@ -169,12 +169,12 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags);
  * must not meet an out-of-memory error in the middle of a run.
  *
  * Same kernels, arguments and results as nnlbm_step, run as plain launches (no CUDA
- * graph).  The per-call scratch of nnlbm_step (the step cursor, the block counter and the
+ * graph).  The per-call scratch of nnlbm_step (the two step cursors and the
  * gathered open-plane node values) lives instead in one file-scope device array of
  * NNLBM_NOALLOC_SCRATCH_BYTES per device.  Its address is looked up the first time this
  * function runs on a device (cudaGetSymbolAddress, with the device current), so that
  * first call should come before any stream capture.  Every call shares the array: the
- * counters are cleared at the start of each group's steps (the node values are written
+ * cursors are cleared at the start of each group's steps (the node values are written
  * before they are read in every step and need no clearing), and calls that overlap in
  * time, from two contexts on one device or from two host threads, race on it.
  *

@@ -69,6 +69,17 @@ const int kChunk = 32;
 const size_t kDfPad = 512;
 const size_t kLabelPad = 64;
 
+// storage for the kernel arguments of either arithmetic type: they hold 64-byte aligned
+// tensor maps, so the bytes are aligned like the structures they stand for
+template <size_t N>
+struct alignas(64) ArgBytes {
+    unsigned char bytes[N];
+    void* data() { return bytes; }
+    const void* data() const { return bytes; }
+};
+constexpr size_t kCaseArgsBytes = std::max(sizeof(CaseArgs<double>), sizeof(CaseArgs<float>));
+constexpr size_t kGroupArgsBytes = std::max(sizeof(GroupArgs<double>), sizeof(GroupArgs<float>));
+
 struct Case {
     nnlbm_case_desc d{};
     int64_t N = 0;
@@ -89,7 +100,7 @@ struct Case {
     // host state
     std::vector<uint8_t> label;      // plain solver labels
     std::vector<uint8_t> dlabel;     // labels with the work flags of the device copy
-    std::vector<int4> chunks;        // {first cell, y | z << 16, 0, first self index}
+    std::vector<Chunk> chunks;       // work list (case index 0)
     std::vector<int32_t> self_cell;  // cells handled by their own thread, in cell order
     std::vector<int32_t> gather_self;// self indices of the gathered nodes
     std::vector<double> self_prof;   // [n_self][3] prescribed velocity of INFLOW_EQ nodes
@@ -101,7 +112,7 @@ struct Case {
     int64_t n_stats = 0;
     bool has_map = false, has_state = false;
     double init[4] = {1.0, 0.0, 0.0, 0.0}; // rho, u of the last initial equilibrium
-    std::vector<char> args;          // CaseArgs<CT>
+    ArgBytes<kCaseArgsBytes> args{}; // CaseArgs<CT>
 };
 
 struct Group {
@@ -109,19 +120,20 @@ struct Group {
     std::vector<int> cases;          // context case indices
     bool dirty = true;
     void* d_cases = nullptr;         // CaseArgs<CT>[n]
-    int4* d_chunks = nullptr;
+    Chunk* d_chunks = nullptr;
     int n_chunks = 0;
     int4* d_gather = nullptr;
+    int2* d_nodes = nullptr;
     int n_gather = 0;
     void* d_bc_prof = nullptr;
     void* d_bc_buf = nullptr;
     int64_t n_self = 0;
-    int* d_ints = nullptr;           // cursor, done
+    int* d_ints = nullptr;           // the two step cursors (one per A-A parity)
     bool any_refd = false;
     int block = 256;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_gen = ~0ull, gen = 0;
-    std::vector<char> args;          // GroupArgs<CT>
+    ArgBytes<kGroupArgsBytes> args{}; // GroupArgs<CT>
 };
 
 } // namespace
@@ -178,10 +190,8 @@ void fill_case_args(const Case& c, CaseArgs<CT>& a)
 void rebuild_case_args(nnlbm_ctx* ctx, Case& c)
 {
     if (c.ct_bytes == 8) {
-        c.args.resize(sizeof(CaseArgs<double>));
         fill_case_args<double>(c, *(CaseArgs<double>*)c.args.data());
     } else {
-        c.args.resize(sizeof(CaseArgs<float>));
         fill_case_args<float>(c, *(CaseArgs<float>*)c.args.data());
     }
     ctx->groups[c.group].dirty = true;
@@ -258,7 +268,9 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
 {
     // per-case argument array and the concatenated work lists of the group
     std::vector<CaseArgs<CT>> ca;
-    std::vector<int4> chunks, gather;
+    std::vector<Chunk> chunks;
+    std::vector<int4> gather;
+    std::vector<int2> nodes;
     std::vector<CT> prof;
     int64_t self_off = 0;
     g.any_refd = false;
@@ -266,25 +278,29 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
         const Case& c = ctx->cases[g.cases[j]];
         ca.push_back(*(const CaseArgs<CT>*)c.args.data());
         g.any_refd |= c.d.cy_mode == NNLBM_CY_REF_FD;
-        for (int4 ch : c.chunks) {
-            ch.z = (int)j | (ch.z & ~CH_CASE_MASK);
-            ch.w += (int)self_off;
+        for (Chunk ch : c.chunks) {
+            ch.cflags = (int)j | (ch.cflags & ~CH_CASE_MASK);
             chunks.push_back(ch);
         }
         for (int32_t k : c.gather_self) gather.push_back(make_int4(c.self_cell[k], (int)j, (int)(self_off + k), 0));
+        for (int32_t cell : c.self_cell) nodes.push_back(make_int2(cell, (int)j));
         for (double v : c.self_prof) prof.push_back((CT)v);
         self_off += (int64_t)c.self_cell.size();
     }
     if (g.d_cases) cudaFree(g.d_cases);
     if (g.d_chunks) cudaFree(g.d_chunks);
     if (g.d_gather) cudaFree(g.d_gather);
+    if (g.d_nodes) cudaFree(g.d_nodes);
+    g.d_nodes = nullptr;
     if (g.d_bc_prof) cudaFree(g.d_bc_prof);
     if (g.d_bc_buf) cudaFree(g.d_bc_buf);
     g.d_cases = nullptr; g.d_chunks = nullptr; g.d_gather = nullptr; g.d_bc_prof = nullptr; g.d_bc_buf = nullptr;
     CK(cudaMalloc(&g.d_cases, std::max<size_t>(ca.size(), 1) * sizeof(CaseArgs<CT>)));
     CK(cudaMemcpy(g.d_cases, ca.data(), ca.size() * sizeof(CaseArgs<CT>), cudaMemcpyHostToDevice));
-    CK(cudaMalloc((void**)&g.d_chunks, std::max<size_t>(chunks.size(), 1) * sizeof(int4)));
-    if (!chunks.empty()) CK(cudaMemcpy(g.d_chunks, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void**)&g.d_chunks, std::max<size_t>(chunks.size(), 1) * sizeof(Chunk)));
+    if (!chunks.empty()) CK(cudaMemcpy(g.d_chunks, chunks.data(), chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void**)&g.d_nodes, std::max<size_t>(nodes.size(), 1) * sizeof(int2)));
+    if (!nodes.empty()) CK(cudaMemcpy(g.d_nodes, nodes.data(), nodes.size() * sizeof(int2), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void**)&g.d_gather, std::max<size_t>(gather.size(), 1) * sizeof(int4)));
     if (!gather.empty()) CK(cudaMemcpy(g.d_gather, gather.data(), gather.size() * sizeof(int4), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&g.d_bc_prof, std::max<size_t>(prof.size(), 1) * sizeof(CT)));
@@ -294,7 +310,6 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     g.n_chunks = (int)chunks.size();
     g.n_gather = (int)gather.size();
     g.n_self = self_off;
-    g.args.resize(sizeof(GroupArgs<CT>));
     GroupArgs<CT>& ga = *(GroupArgs<CT>*)g.args.data();
     memset(&ga, 0, sizeof ga);
     ga.c0 = ca[0];
@@ -304,10 +319,11 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     ga.n_chunks = g.n_chunks;
     ga.gather = g.d_gather;
     ga.n_gather = g.n_gather;
+    ga.nodes = g.d_nodes;
+    ga.n_nodes = (int)g.n_self;
     ga.bc_prof = (const CT*)g.d_bc_prof;
     ga.bc_buf = (CT*)g.d_bc_buf;
     ga.cursor = g.d_ints;
-    ga.done = g.d_ints + 1;
     g.dirty = false;
     g.gen++;
     return NNLBM_OK;
@@ -319,12 +335,15 @@ int prepare_group(nnlbm_ctx* ctx, Group& g)
     return g.dtype == NNLBM_F64 ? upload_group<double>(ctx, g) : upload_group<float>(ctx, g);
 }
 
+// warps of one step launch: one per chunk, then one per 32 boundary nodes
+int step_warps(const Group& g) { return std::max(g.n_chunks + (int)((g.n_self + 31) / 32), 1); }
+
 // enqueue one step of a group (no host synchronisation); `odd` is the A-A parity
 int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
 {
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
-    const dim3 cgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block), cblk(g.block);
+    const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
     if (g.any_refd) {
         A.refd_velocity(odd, cgrid, cblk, ctx->stream, g.args.data());
         A.refd_stress(odd, cgrid, cblk, ctx->stream, g.args.data());
@@ -415,13 +434,14 @@ int wait_and_check(nnlbm_ctx* ctx, int64_t n)
     for (size_t i = 0; i < ctx->cases.size(); ++i)
         CK(cudaMemcpyAsync(&err[i], ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    for (size_t i = 0; i < ctx->groups.size(); ++i)
-        if (cur[2 * i] != n)
-            return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", i, cur[2 * i], (long long)n);
-    for (size_t i = 0; i < ctx->cases.size(); ++i) {
-        if (err[i] & 2) return set_err(ctx, NNLBM_ERR_TIMEOUT, "case %zu: a staged chunk did not arrive in time", i);
-        if (err[i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
+    for (size_t i = 0; i < ctx->groups.size(); ++i) {
+        // the last step stored n into the cursor of the parity the group is at now
+        const int k = 2 * (int)i + (int)(ctx->cases[ctx->groups[i].cases[0]].parity & 1);
+        if (cur[k] != n)
+            return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", i, cur[k], (long long)n);
     }
+    for (size_t i = 0; i < ctx->cases.size(); ++i)
+        if (err[i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
     return NNLBM_OK;
 }
 
@@ -463,8 +483,8 @@ size_t canon_index(const Case& c, int x, int y, int z, int q, int* slot)
 
 // ---------------------------------------------------------------------------------------
 // scratch of nnlbm_step_noalloc: one file-scope device array per device (the module's
-// global), never allocated or freed by this library.  Layout: [0, 256) the step cursor and
-// the block counter of the step kernel, then the gathered open-plane node values
+// global), never allocated or freed by this library.  Layout: [0, 256) the two step
+// cursors of the step kernels (one per A-A parity), then the gathered open-plane node values
 // (rho, ux, uy, uz per node) of the launch group being stepped.
 // ---------------------------------------------------------------------------------------
 constexpr size_t kNoallocHead = 256;
@@ -533,7 +553,6 @@ void noalloc_args(const Group& g, char* scratch, char* out)
     GroupArgs<CT>& ga = *(GroupArgs<CT>*)out;
     memcpy(&ga, g.args.data(), sizeof ga);
     ga.cursor = (int*)scratch;
-    ga.done = (int*)scratch + 1;
     ga.bc_buf = (CT*)(scratch + kNoallocHead);
 }
 
@@ -638,61 +657,48 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 neq += lab == L_IN_EQ;
                 nbc += lab >= L_IN_L;
             }
-    // work flags: which open-plane nodes are finished by the thread of their inward
-    // neighbour (same stencil, same force) and which need their own thread
+    // boundary nodes (open planes and GEO_INFLOW cells), in cell order: each is written by
+    // its own lane of the node warps; the open-plane ones are gathered first
     std::vector<uint8_t> dl(map, map + c.N);
-    for (int z = 0; z < nz; ++z)
-        for (int y = 0; y < ny; ++y)
-            for (int x = 0; x < nx; ++x) {
-                const size_t i = id(x, y, z);
-                const int lab = map[i];
-                if (lab == L_IN_EQ) { dl[i] |= LF_SELF; continue; }
-                if (!is_pull_bc(lab)) continue;
-                const bool xnormal = lab == L_IN_L || lab == L_IN_R || lab == L_OUT_REQ;
-                const bool tangential_interior = xnormal ? (y > 0 && y < ny - 1 && z > 0 && z < nz - 1)
-                                                         : (x > 0 && x < nx - 1 && z > 0 && z < nz - 1);
-                int sx = x, sy = y;
-                if (lab == L_IN_L) sx = x + 1;
-                if (lab == L_IN_R || lab == L_OUT_REQ) sx = x - 1;
-                if (lab == L_OUT_F) sy = y + 1;
-                if (lab == L_OUT_B) sy = y - 1;
-                const int sl = map[id(sx, sy, z)];
-                const bool src_ok = sl == L_FLUID || sl == L_PERIODIC;
-                // under CY_REF_FD the source's velocity carries its own CY force
-                const bool force_ok = c.d.cy_mode != NNLBM_CY_REF_FD || lab == L_IN_L || lab == L_IN_R;
-                if (tangential_interior && src_ok && force_ok) {
-                    dl[i] |= LF_FUSED;
-                    dl[id(sx, sy, z)] |= LF_SOURCE;
-                } else {
-                    dl[i] |= LF_SELF;
-                }
-            }
-    // packed work list of 32-cell row chunks and the self-handled nodes: a chunk starts at
-    // the first cell with work not yet covered in its row, so a short row segment fills
-    // one chunk instead of straddling two
-    std::vector<int4> chunks;
     std::vector<int32_t> self_cell, gather_self;
-    auto has_work = [&](size_t i) { return map[i] == L_FLUID || map[i] == L_PERIODIC || (dl[i] & LF_SELF); };
+    for (size_t i = 0; i < (size_t)c.N; ++i) {
+        const int lab = map[i];
+        if (lab != L_IN_EQ && !is_pull_bc(lab)) continue;
+        dl[i] |= LF_SELF;
+        if (lab != L_IN_EQ) gather_self.push_back((int32_t)self_cell.size());
+        self_cell.push_back((int32_t)i);
+    }
+    // packed work list of 32-cell row chunks of colliding cells: a chunk starts at the first
+    // colliding cell not yet covered in its row, rounded down to a 32-byte boundary of the
+    // population rows (but not into the previous chunk), so that a short row segment fills
+    // one chunk instead of straddling two and each row load touches as few sectors as it can
+    std::vector<Chunk> chunks;
+    auto collides = [&](size_t i) { return map[i] == L_FLUID || map[i] == L_PERIODIC; };
+    const int align = 32 / kStorageBytes[c.d.dtype];
     for (int z = 0; z < nz; ++z)
         for (int y = 0; y < ny; ++y)
-            for (int x0 = 0; x0 < nx; x0 += kChunk) {
-                while (x0 < nx && !has_work(id(x0, y, z))) ++x0;
+            for (int x0 = 0, end = 0; x0 < nx; x0 += kChunk, end = x0) {
+                while (x0 < nx && !collides(id(x0, y, z))) ++x0;
                 if (x0 >= nx) break;
-                const int self_base = (int)self_cell.size();
-                bool work = false, fluid = false;
+                x0 = std::max(x0 / align * align, end);
+                Chunk ch{};
+                ch.c0 = (int)id(x0, y, z);
+                ch.yz = y | (z << 16);
                 for (int x = x0; x < std::min(nx, x0 + kChunk); ++x) {
                     const size_t i = id(x, y, z);
-                    const int lab = map[i];
-                    if (lab == L_FLUID || lab == L_PERIODIC) work = fluid = true;
-                    if (dl[i] & LF_SELF) {
-                        work = true;
-                        if (lab != L_IN_EQ) gather_self.push_back((int32_t)self_cell.size());
-                        self_cell.push_back((int32_t)i);
+                    const unsigned bit = 1u << (x - x0);
+                    if (collides(i)) {
+                        ch.fluid |= bit;
+                        if (map[i] == L_PERIODIC) ch.periodic |= bit;
                     }
                 }
-                // flags: the chunk has colliding cells; the chunk lies on a y or z face
-                const int fl = (fluid ? CH_FLUID : 0) | (y == 0 || y == ny - 1 || z == 0 || z == nz - 1 ? CH_FACE : 0);
-                if (work) chunks.push_back(make_int4((int)id(x0, y, z), y | (z << 16), fl, self_base));
+                // flags: the chunk lies on a y or z face; the chunk is plain (no colliding cell
+                // on an x face either, so no neighbour index wraps)
+                const bool face = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
+                const unsigned xface = (x0 == 0 ? 1u : 0u) | (nx - 1 - x0 < kChunk ? 1u << (nx - 1 - x0) : 0u);
+                const bool plain = !face && !(ch.fluid & xface);
+                ch.cflags = CH_FLUID | (face ? CH_FACE : 0) | (plain ? CH_PLAIN : 0);
+                chunks.push_back(ch);
             }
     c.label.assign(map, map + c.N);
     c.dlabel = dl;
@@ -1070,7 +1076,7 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
     if ((rc = prepare_steps(ctx, g, n_steps, flags)) != NNLBM_OK) return rc;
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
-    const dim3 cgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block), cblk(g.block);
+    const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
     for (int i = 0; i < 5; ++i) { ms[i] = 0; launches[i] = 0; }
     const int64_t parity = ctx->cases[g.cases[0]].parity;
     // kinds: 0 gather, 1 step, 3 CY_REF_FD velocity, 4 CY_REF_FD strain
@@ -1165,15 +1171,15 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
             if (rc != NNLBM_OK) return rc;
             if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
         }
-        // the two counters start at zero for every group; the group's steps, in stream
+        // the two cursors start at zero for every group; the group's steps, in stream
         // order, finish before the next group clears them again
         CK(cudaMemsetAsync(scratch, 0, 2 * sizeof(int), ctx->stream));
-        alignas(16) char args[sizeof(GroupArgs<double>)];
+        alignas(64) char args[kGroupArgsBytes];
         if (f64) noalloc_args<double>(g, scratch, args);
         else noalloc_args<float>(g, scratch, args);
         const AuxLaunchers& A = aux_launchers(g.dtype);
         const int per_block = g.block / kChunk;
-        const dim3 cgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block), cblk(g.block);
+        const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
         const int64_t parity = ctx->cases[g.cases[0]].parity;
         for (int64_t k = 0; k < n_steps; ++k) {
             const bool odd = ((parity + k) & 1) != 0;
@@ -1185,8 +1191,10 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
             step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, args);
         }
         CK(cudaGetLastError());
-        // pageable destination: the copy returns once the cursor is on the host
-        CK(cudaMemcpyAsync(&cursors[gi], scratch, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        // pageable destination: the copy returns once the cursor is on the host; the last
+        // step stored n_steps into the cursor of the parity after it
+        CK(cudaMemcpyAsync(&cursors[gi], (int*)scratch + ((parity + n_steps) & 1), sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
         finish_steps(ctx, g, n_steps, flags);
     }
     for (Case& c : ctx->cases) {
@@ -1202,7 +1210,6 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
                            (long long)n_steps);
     for (size_t i = 0; i < ctx->cases.size(); ++i) {
         CK(cudaMemcpy(&err, ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (err & 2) return set_err(ctx, NNLBM_ERR_TIMEOUT, "case %zu: a staged chunk did not arrive in time", i);
         if (err) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
     }
     return NNLBM_OK;
@@ -1228,7 +1235,7 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
     for (Group& g : ctx->groups) {
         for (int p = 0; p < 2; ++p)
             if (g.graph[p]) cudaGraphExecDestroy(g.graph[p]);
-        void* ptrs[] = {g.d_cases, g.d_chunks, g.d_gather, g.d_bc_prof, g.d_bc_buf, g.d_ints};
+        void* ptrs[] = {g.d_cases, g.d_chunks, g.d_gather, g.d_nodes, g.d_bc_prof, g.d_bc_buf, g.d_ints};
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }

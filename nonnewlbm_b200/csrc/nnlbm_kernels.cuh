@@ -34,7 +34,6 @@
 #include <stdint.h>
 
 #include <algorithm>
-#include <atomic>
 
 #include "nnlbm_physics.cuh"
 
@@ -42,8 +41,9 @@ namespace nnlbm {
 
 enum : int { L_FLUID = 0, L_WALL = 1, L_PERIODIC = 2, L_IN_L = 3, L_IN_R = 4, L_OUT_F = 5, L_OUT_B = 6,
              L_IN_EQ = 7, L_OUT_REQ = 8 };
-// flag bits of the device label byte (the low four bits hold the label)
-enum : int { LF_SOURCE = 0x80, LF_SELF = 0x40, LF_FUSED = 0x20, L_MASK = 0x0f };
+// flag bit of the device label byte (the low four bits hold the label): a boundary node
+// of the node list
+enum : int { LF_SELF = 0x40, L_MASK = 0x0f };
 enum : int { CY_NONE = 0, CY_REF_FD = 1, CY_LOCAL_NEQ = 2 };
 enum : int { F_STATS = 1, F_MACRO = 2, F_REDUCE = 4 };
 // macro field order of the context's macro array
@@ -57,26 +57,26 @@ template <int DT> struct Storage;
 template <> struct Storage<0> {
     using T = double; using CT = double;
     __device__ static __forceinline__ CT from(T v, int, CT) { return v; }
-    __device__ static __forceinline__ CT load(const T* p, int i, int, CT) { return p[i]; }
-    __device__ static __forceinline__ void store(T* p, int i, int, CT v, CT) { p[i] = v; }
+    __device__ static __forceinline__ CT load(const T* p, int64_t i, int, CT) { return p[i]; }
+    __device__ static __forceinline__ void store(T* p, int64_t i, int, CT v, CT) { p[i] = v; }
 };
 template <> struct Storage<1> {
     using T = float; using CT = float;
     __device__ static __forceinline__ CT from(T v, int q, CT) { return weight<float>(q) + v; }
-    __device__ static __forceinline__ CT load(const T* p, int i, int q, CT) { return weight<float>(q) + p[i]; }
-    __device__ static __forceinline__ void store(T* p, int i, int q, CT v, CT) { p[i] = v - weight<float>(q); }
+    __device__ static __forceinline__ CT load(const T* p, int64_t i, int q, CT) { return weight<float>(q) + p[i]; }
+    __device__ static __forceinline__ void store(T* p, int64_t i, int q, CT v, CT) { p[i] = v - weight<float>(q); }
 };
 template <> struct Storage<2> {
     using T = __half; using CT = float;
     __device__ static __forceinline__ CT from(T v, int q, CT isc) { return weight<float>(q) + __half2float(v) * isc; }
-    __device__ static __forceinline__ CT load(const T* p, int i, int q, CT isc) { return from(p[i], q, isc); }
-    __device__ static __forceinline__ void store(T* p, int i, int q, CT v, CT sc) { p[i] = __float2half_rn((v - weight<float>(q)) * sc); }
+    __device__ static __forceinline__ CT load(const T* p, int64_t i, int q, CT isc) { return from(p[i], q, isc); }
+    __device__ static __forceinline__ void store(T* p, int64_t i, int q, CT v, CT sc) { p[i] = __float2half_rn((v - weight<float>(q)) * sc); }
 };
 template <> struct Storage<3> {
     using T = __nv_bfloat16; using CT = float;
     __device__ static __forceinline__ CT from(T v, int q, CT isc) { return weight<float>(q) + __bfloat162float(v) * isc; }
-    __device__ static __forceinline__ CT load(const T* p, int i, int q, CT isc) { return from(p[i], q, isc); }
-    __device__ static __forceinline__ void store(T* p, int i, int q, CT v, CT sc) { p[i] = __float2bfloat16_rn((v - weight<float>(q)) * sc); }
+    __device__ static __forceinline__ CT load(const T* p, int64_t i, int q, CT isc) { return from(p[i], q, isc); }
+    __device__ static __forceinline__ void store(T* p, int64_t i, int q, CT v, CT sc) { p[i] = __float2bfloat16_rn((v - weight<float>(q)) * sc); }
 };
 
 // per-step control row written by the host before each nnlbm_step call and indexed by a
@@ -109,20 +109,34 @@ struct CaseArgs {
     int* err;                  // watchdog flag
 };
 
+// one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
+// and per lane (bit = lane) which cells collide and which of those are PERIODIC
+struct alignas(16) Chunk {
+    int c0, yz, cflags, pad0;
+    unsigned fluid, periodic, pad1, pad2;
+};
+// chunk flags (bits 16.. of cflags, the case index below).  CH_PLAIN: no neighbour of any
+// colliding lane wraps around the box (the chunk is off the y/z faces and has no
+// colliding cell at x = 0 or nx-1)
+enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PLAIN = 1 << 18 };
+
 // a launch group: cases sharing storage type and collision
 template <class CT>
 struct GroupArgs {
     CaseArgs<CT> c0;           // copy of case 0 in parameter space (single-case groups)
     int n_cases, pad2;
     const CaseArgs<CT>* cases;
-    const int4* chunks;        // {first cell, y | z << 16, case, first self-node index}
+    const Chunk* chunks;
     int n_chunks, pad0;
-    const int4* gather;        // {cell, case, self-node index, 0} of the gathered nodes
-    int n_gather, pad1;
-    const CT* bc_prof;         // [n_self][3] prescribed velocity (GEO_INFLOW nodes)
-    CT* bc_buf;                // [n_self][4] gathered rho, ux, uy, uz
-    int* cursor;               // step cursor into every case's ctl
-    int* done;                 // block counter of the step kernel
+    const int4* gather;        // {cell, case, node index, 0} of the open-plane nodes
+    int n_gather, n_nodes;
+    const int2* nodes;         // [n_nodes] {cell, case} of every boundary node (open planes, INFLOW_EQ)
+    const CT* bc_prof;         // [n_nodes][3] prescribed velocity (GEO_INFLOW nodes)
+    CT* bc_buf;                // [n_nodes][4] gathered rho, ux, uy, uz
+    // step cursors into every case's ctl, one per A-A parity: a step of parity p reads
+    // cursor[p] and stores cursor[p] + 1 into cursor[1 - p], which no kernel of the step
+    // reads, so no launch needs a grid-wide count
+    int* cursor;
 };
 
 template <int DT>
@@ -220,23 +234,14 @@ __device__ __forceinline__ double node_outputs(const CaseArgs<CT>& a, int flags,
     return lab == L_IN_L ? (double)ux : lab == L_IN_R ? -(double)ux : lab == L_OUT_F ? -(double)uy : lab == L_OUT_B ? (double)uy : 0.0;
 }
 
-// rare paths of the step kernel are kept out of line so that they do not take registers
-// from the bulk path: the equilibrium of an open-plane node with its bookkeeping ...
-template <int DT, bool ODD>
-__device__ __noinline__ double finish_node(const CaseArgs<typename Storage<DT>::CT>& a, int flags, int lab, int c, int x, int y,
-                                           int z, typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
-                                           typename Storage<DT>::CT uy, typename Storage<DT>::CT uz)
-{
-    store_node_eq<DT, ODD>(a, c, x, y, z, rho, ux, uy, uz);
-    return node_outputs<typename Storage<DT>::CT>(a, flags, lab, c, rho, ux, uy, uz);
-}
-
-// ... and the finite-difference Carreau-Yasuda force of CY_REF_FD (core.h:663-781):
+// the finite-difference Carreau-Yasuda force of CY_REF_FD (core.h:663-781), kept out of
+// line so that it takes no registers from the bulk path:
 // divergence of the strain of the previous phase with one-sided differences next to
 // non-FLUID cells, then 2 (nu(gamma) - nu) F rho with rho still at its default of 1
 template <class CT>
-__device__ __noinline__ void refd_force(const CaseArgs<CT>& a, int c, int sy, int sz, CT* F)
+__device__ __noinline__ void refd_force(const CaseArgs<CT>* ap, int c, int sy, int sz, CT* F)
 {
+    const CaseArgs<CT>& a = *ap;
     const CT* M = a.macro;
     const int64_t N = a.N;
     const int cn[6] = {c - 1, c + 1, c - sy, c + sy, c - sz, c + sz};
@@ -273,217 +278,73 @@ struct StepOccupancy {
 };
 
 // ---------------------------------------------------------------------------------------
-// shared-memory staging of a chunk with TMA bulk copies (cp.async.bulk global -> shared,
-// completion counted in bytes on an mbarrier); no cluster, no multicast
+// one 32-cell chunk of the fused step (solver/lbm3d/core.h:578-800), one warp, one cell per
+// lane.  The populations go straight from HBM to registers, 27 coalesced row loads per
+// warp, issued as soon as the chunk record is in (its lane masks say which lanes collide,
+// so no label load sits in front of them).  On a plain chunk every address is the cell's
+// pointer plus an offset made of the slot, row and plane strides only; the rare chunks on
+// a face wrap their neighbour indices around the box.
 // ---------------------------------------------------------------------------------------
-// chunk record flags (bits 16.. of the case word)
-enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-// one bounded probe of the phase; the hint caps the suspension at 20 microseconds
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
-{
-    uint32_t done;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(done)
-                 : "r"(bar), "r"(parity), "r"(20000u)
-                 : "memory");
-    return done != 0;
-}
-
-// wait for a phase with an iteration limit (about two seconds); false when it ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-    for (int it = 0; it < 100000; ++it)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-// `bytes` (a multiple of 16) from 16-byte aligned global memory into shared memory
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-// one pipeline stage of a warp: the 27 population rows of its chunk, each copied from the
-// 16-byte boundary at or below the row's first element (so a row spans 32 elements plus
-// up to 16 bytes of slack), and the chunk's label row likewise
-template <int DT>
-struct Stage {
-    static constexpr int S = (int)sizeof(typename Storage<DT>::T);
-    static constexpr int RB = 32 * S + 16;
-    static constexpr int LB = 48;
-    static constexpr int BYTES = 27 * RB + LB;
-};
-// per warp: two mbarriers (16 B) and a ring of its next 32 chunk records (512 B), then
-// the two stages; up to 8 warps per block
-constexpr int kRing = 32;
-constexpr int kStepSmemHead = 8 * (16 + kRing * 16);
-template <int DT>
-constexpr int step_smem_bytes(int warps_per_block) { return kStepSmemHead + warps_per_block * 2 * Stage<DT>::BYTES; }
-
-// start the copies of chunk `rec` into stage `stg`; returns the bytes the stage's
-// mbarrier expects (0: the chunk loads directly from global memory)
-template <int DT, bool ODD, bool SINGLE>
-__device__ __forceinline__ uint32_t issue_chunk(const GroupArgs<typename Storage<DT>::CT>& g, int4 rec, unsigned char* stg,
-                                                uint32_t bar, int lane)
-{
-    using G = Stage<DT>;
-    using CT = typename Storage<DT>::CT;
-    // an odd step of a chunk on a y/z face pulls across the face (wrapped rows)
-    if (ODD && (rec.z & CH_FACE)) return 0;
-    const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[rec.z & CH_CASE_MASK];
-    const bool fluid = (rec.z & CH_FLUID) != 0;
-    const uint32_t bytes = fluid ? (uint32_t)(27 * G::RB + G::LB) : (uint32_t)G::LB;
-    if (lane == 0) mbar_arrive_expect_tx(bar, bytes);
-    __syncwarp();
-    const int c0 = rec.x;
-    if (lane < 27) {
-        if (fluid) {
-            const int q = lane;
-            // even: slot q at the chunk's cells; odd: slot opp(q) at the cells - c_q
-            const int slot = ODD ? oppq(q) : q;
-            const int cs = ODD ? c0 - (cxq(q) + a.nx * cyq(q) + a.nx * a.ny * czq(q)) : c0;
-            const int64_t off = ((int64_t)slot * a.qstride + cs) * G::S;
-            bulk_g2s(smem_u32(stg) + q * G::RB, (const char*)a.df + (off & ~(int64_t)15), G::RB, bar);
-        }
-    } else if (lane == 27) {
-        bulk_g2s(smem_u32(stg) + 27 * G::RB, a.label + (c0 & ~15), G::LB, bar);
-    }
-    return bytes;
-}
-
-// ---------------------------------------------------------------------------------------
-// one 32-cell chunk of the fused step (solver/lbm3d/core.h:578-800): FLUID / PERIODIC
-// cells collide, source cells also finish their fused open-plane neighbours,
-// self-handled nodes write their equilibrium.  `stg` is the chunk's staged rows, or null
-// when the chunk loads directly from global memory.
-// ---------------------------------------------------------------------------------------
-template <int DT, int COL, bool ODD, bool SINGLE>
-__device__ __forceinline__ void process_chunk(const GroupArgs<typename Storage<DT>::CT>& g, int4 ch, const unsigned char* stg,
-                                              int step, int lane)
+template <int DT, int COL, bool ODD>
+__device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>::CT>& a, const CaseArgs<typename Storage<DT>::CT>* ap,
+                                            const Chunk& ch, int flags, int lane)
 {
     using S = Storage<DT>;
     using T = typename S::T;
     using CT = typename S::CT;
-    using G = Stage<DT>;
-    const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[ch.z & CH_CASE_MASK];
-    const int y = ch.y & 0xffff, z = ch.y >> 16;
-    const int sy = a.nx, sz = a.nx * a.ny;
-    const int x0 = ch.x - y * sy - z * sz;
-    const int x = x0 + lane;
-    const bool inb = x < a.nx;
-    const int c = ch.x + lane;
-    const int raw = !inb ? (int)L_WALL : stg ? (int)stg[27 * G::RB + (ch.x & 15) + lane] : (int)a.label[c];
-    const int lab = raw & L_MASK;
-    const bool fluid = lab == L_FLUID || lab == L_PERIODIC;
-    const bool self = (raw & LF_SELF) != 0;
-    const unsigned selfmask = __ballot_sync(0xffffffffu, self);
-    const int flags = a.ctl[step].flags;
-    double mass = 0.0, q3 = 0.0, q4 = 0.0, q5 = 0.0, q6 = 0.0;
-    if (fluid) {
-        const bool xin = x > 0 && x < a.nx - 1;
-        // odd steps: index corrections of the wrapped neighbours (zero inside the box);
-        // w*m apply to a neighbour at coordinate - 1, w*p to one at coordinate + 1
-        const int wxm = x == 0 ? a.nx : 0, wxp = x == a.nx - 1 ? -a.nx : 0;
-        const int wym = y == 0 ? sz : 0, wyp = y == a.ny - 1 ? -sz : 0;
-        const int wzm = z == 0 ? (int)a.N : 0, wzp = z == a.nz - 1 ? -(int)a.N : 0;
-        auto nbr = [&](int q, int sign) -> int { // cell at x + sign c_q
-            const int dx = sign * cxq(q), dy = sign * cyq(q), dz = sign * czq(q);
-            return c + dx + sy * dy + sz * dz + (dx < 0 ? wxm : dx > 0 ? wxp : 0) + (dy < 0 ? wym : dy > 0 ? wyp : 0) +
-                   (dz < 0 ? wzm : dz > 0 ? wzp : 0);
+    double mass = 0.0;
+    const unsigned bit = 1u << lane;
+    if (ch.fluid & bit) {
+        const int c = ch.c0 + lane;
+        const int64_t qs = a.qstride, sy = a.nx, sz = (int64_t)a.nx * a.ny;
+        const bool plain = (ch.cflags & CH_PLAIN) != 0;
+        // the wrapped neighbour cell x + sign c_q of a face chunk
+        auto nbr = [&](int q, int sign) -> int64_t {
+            const int y = ch.yz & 0xffff, z = ch.yz >> 16;
+            const int x = ch.c0 - y * a.nx - z * a.nx * a.ny + lane;
+            return (int64_t)wrapc(x + sign * cxq(q), a.nx) + sy * wrapc(y + sign * cyq(q), a.ny) +
+                   sz * wrapc(z + sign * czq(q), a.nz) - c;
         };
+        const T* pc = (const T*)a.df + c;
         CT f[27];
         if (!ODD) {
-            // even steps always have the chunk staged: the element of this lane sits
-            // (first element mod 16) bytes into its row, plus lane * element size
-            const unsigned char* p = stg + lane * G::S + (((unsigned)ch.x * (unsigned)G::S) & 15u);
+            // slot q at c
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = S::from(*(const T*)(p + q * G::RB), q, a.inv_scale);
-        } else if (stg && xin) {
-            const unsigned char* p = stg + lane * G::S;
-            const unsigned c0b = (unsigned)ch.x * (unsigned)G::S;
-            const unsigned syb = (unsigned)sy * (unsigned)G::S, szb = (unsigned)sz * (unsigned)G::S;
+            for (int q = 0; q < 27; ++q) f[q] = S::from(pc[q * qs], q, a.inv_scale);
+        } else if (plain) {
+            // slot opp(q) at c - c_q
 #pragma unroll
-            for (int q = 0; q < 27; ++q) {
-                const unsigned d = (c0b - (unsigned)(cxq(q) * G::S) - (unsigned)cyq(q) * syb - (unsigned)czq(q) * szb) & 15u;
-                f[q] = S::from(*(const T*)(p + q * G::RB + d), q, a.inv_scale);
-            }
+            for (int q = 0; q < 27; ++q)
+                f[q] = S::from(pc[oppq(q) * qs - (cxq(q) + cyq(q) * sy + czq(q) * sz)], q, a.inv_scale);
         } else {
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = S::load(qptr<DT>(a, oppq(q)), nbr(q, -1), q, a.inv_scale);
+            for (int q = 0; q < 27; ++q) f[q] = S::from(pc[oppq(q) * qs + nbr(q, -1)], q, a.inv_scale);
         }
         CT fx = a.fx, fy = a.fy, fz = a.fz;
-        if (a.cy_mode == CY_REF_FD && lab == L_FLUID) {
+        if (a.cy_mode == CY_REF_FD && !(ch.periodic & bit)) {
             CT F[3] = {fx, fy, fz};
-            refd_force<CT>(a, c, sy, sz, F);
+            refd_force<CT>(ap, c, (int)sy, (int)sz, F);
             fx = F[0]; fy = F[1]; fz = F[2];
         }
         CT rho, ux, uy, uz;
         density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
-        if (raw & LF_SOURCE) {
-            // fused open-plane neighbours: their re-centred stencil is this cell's own pull
-            const StepCtl<CT>& ctl = a.ctl[step];
-            const int nbc[4] = {c - 1, c + 1, c - sy, c + sy};
-            const bool inside[4] = {x > 0, x < a.nx - 1, y > 0, y < a.ny - 1};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (!inside[k]) continue;
-                const int nr = a.label[nbc[k]];
-                const int nl = nr & L_MASK;
-                const bool ok = (nr & LF_FUSED) && (k == 0 ? nl == L_IN_L : k == 1 ? (nl == L_IN_R || nl == L_OUT_REQ)
-                                                                           : k == 2 ? nl == L_OUT_F : nl == L_OUT_B);
-                if (!ok) continue;
-                const int bx = x + (k == 0 ? -1 : k == 1 ? 1 : 0), by = y + (k == 2 ? -1 : k == 3 ? 1 : 0);
-                CT brho, bux = 0, buy = 0, buz = 0;
-                if (nl == L_IN_L || nl == L_IN_R) { // sim_tcpc.cu:242-261
-                    brho = rho;
-                    bux = nl == L_IN_L ? ctl.u_left : ctl.u_right;
-                } else { // sim_tcpc.cu:262-273, lbm_bc.h:147-152
-                    brho = CT(1); bux = ux; buy = uy; buz = uz;
-                }
-                const double qn = finish_node<DT, ODD>(a, flags, nl, nbc[k], bx, by, z, brho, bux, buy, buz);
-                if (nl == L_IN_L) q3 += qn;
-                else if (nl == L_IN_R) q4 += qn;
-                else if (nl == L_OUT_F) q5 += qn;
-                else if (nl == L_OUT_B) q6 += qn;
-            }
-        }
         // one inlined collision for both viscosity models (the local Carreau-Yasuda law is
         // a runtime branch inside it)
         CT Sl[6];
         const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
         collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
-        // one running pointer over the direction arrays keeps the 27 store addresses out
-        // of the register file
-        const int64_t qs = a.qstride;
+        T* ps = (T*)a.df + c;
         if (!ODD) {
-            T* p = (T*)a.df + (c + 26 * qs);
+            // slot opp(q) at c
 #pragma unroll
-            for (int q = 0; q < 27; ++q, p -= qs) S::store(p, 0, q, f[q], a.scale);
+            for (int q = 0; q < 27; ++q) S::store(ps, oppq(q) * qs, q, f[q], a.scale);
+        } else if (plain) {
+            // slot q at c + c_q
+#pragma unroll
+            for (int q = 0; q < 27; ++q) S::store(ps, q * qs + (cxq(q) + cyq(q) * sy + czq(q) * sz), q, f[q], a.scale);
         } else {
-            T* p = (T*)a.df;
 #pragma unroll
-            for (int q = 0; q < 27; ++q, p += qs) S::store(p, nbr(q, 1), q, f[q], a.scale);
+            for (int q = 0; q < 27; ++q) S::store(ps, q * qs + nbr(q, 1), q, f[q], a.scale);
         }
         if ((flags & F_MACRO) || a.cy_mode == CY_REF_FD) {
             write_macro<CT>(a, c, rho, ux, uy, uz, fx, fy, fz);
@@ -495,110 +356,65 @@ __device__ __forceinline__ void process_chunk(const GroupArgs<typename Storage<D
         if (flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
         if (!(rho > CT(0.25) && rho < CT(4))) atomicOr(a.err, 1);
         mass = (double)rho;
-    } else if (self) {
-        // GEO_INFLOW nodes (lbm_bc.h:126-129) and gathered open-plane nodes
-        const int k = ch.w + __popc(selfmask & ((1u << lane) - 1u));
-        CT rho, ux, uy, uz;
-        if (lab == L_IN_EQ) {
-            const StepCtl<CT>& ctl = a.ctl[step];
-            rho = ctl.rho_eq;
-            ux = g.bc_prof[3 * k] * ctl.prof_scale;
-            uy = g.bc_prof[3 * k + 1] * ctl.prof_scale;
-            uz = g.bc_prof[3 * k + 2] * ctl.prof_scale;
-        } else {
-            rho = g.bc_buf[4 * k]; ux = g.bc_buf[4 * k + 1]; uy = g.bc_buf[4 * k + 2]; uz = g.bc_buf[4 * k + 3];
-        }
-        const double qn = finish_node<DT, ODD>(a, flags, lab, c, x, y, z, rho, ux, uy, uz);
-        if (lab == L_IN_L) q3 = qn;
-        else if (lab == L_IN_R) q4 = qn;
-        else if (lab == L_OUT_F) q5 = qn;
-        else if (lab == L_OUT_B) q6 = qn;
     }
     if (flags & F_REDUCE) {
-        const double s0 = warp_sum(mass), s1 = warp_sum(q3), s2 = warp_sum(q4), s3 = warp_sum(q5), s4 = warp_sum(q6);
-        if (lane == 0) {
-            if (s0 != 0.0) atomicAdd(a.red, s0);
-            if (s1 != 0.0) atomicAdd(a.red + 1, s1);
-            if (s2 != 0.0) atomicAdd(a.red + 2, s2);
-            if (s3 != 0.0) atomicAdd(a.red + 3, s3);
-            if (s4 != 0.0) atomicAdd(a.red + 4, s4);
-        }
+        const double s0 = warp_sum(mass);
+        if (lane == 0 && s0 != 0.0) atomicAdd(a.red, s0);
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// the step kernel: persistent warps walk the chunk list with a stride of all warps of the
-// grid; each warp stages its next chunk in shared memory (two stages) while it computes
-// the current one.  The last block to finish advances the step cursor.
-// ---------------------------------------------------------------------------------------
+// 32 boundary nodes (open-plane nodes and GEO_INFLOW nodes, one per lane): each writes
+// the equilibrium of its gathered (rho, u) (or of its prescribed inflow) into its own
+// slots, which no other cell reads or writes within the step, and adds its plane flux
+template <int DT, bool ODD>
+__device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const CaseArgs<typename Storage<DT>::CT>* cases,
+                                        const typename Storage<DT>::CT* bc_prof, const typename Storage<DT>::CT* bc_buf, int k,
+                                        int step, int flags)
+{
+    using CT = typename Storage<DT>::CT;
+    if (k >= n_nodes) return;
+    const int2 nd = nodes[k];
+    const CaseArgs<CT>& a = cases[nd.y];
+    const int c = nd.x;
+    const int lab = a.label[c] & L_MASK;
+    const int x = c % a.nx, y = (c / a.nx) % a.ny, z = c / (a.nx * a.ny);
+    CT rho, ux, uy, uz;
+    if (lab == L_IN_EQ) { // lbm_bc.h:126-129
+        const StepCtl<CT>& ctl = a.ctl[step];
+        rho = ctl.rho_eq;
+        ux = bc_prof[3 * k] * ctl.prof_scale;
+        uy = bc_prof[3 * k + 1] * ctl.prof_scale;
+        uz = bc_prof[3 * k + 2] * ctl.prof_scale;
+    } else {
+        rho = bc_buf[4 * k]; ux = bc_buf[4 * k + 1]; uy = bc_buf[4 * k + 2]; uz = bc_buf[4 * k + 3];
+    }
+    store_node_eq<DT, ODD>(a, c, x, y, z, rho, ux, uy, uz);
+    const double qn = node_outputs<CT>(a, flags, lab, c, rho, ux, uy, uz);
+    if ((flags & F_REDUCE) && qn != 0.0) {
+        const int slot = lab == L_IN_L ? 1 : lab == L_IN_R ? 2 : lab == L_OUT_F ? 3 : lab == L_OUT_B ? 4 : 0;
+        if (slot) atomicAdd(a.red + slot, qn);
+    }
+}
+
+// the step kernel: one warp per chunk of the work list, then one warp per 32 boundary
+// nodes.  Both write only the slots their own cells read, so they run side by side.
 template <int DT, int COL, bool ODD, bool SINGLE>
 __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
     k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
-    using G = Stage<DT>;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-    const uint32_t bar0 = smem_u32(smem) + 16 * wib;
-    int4* const ring = (int4*)(smem + 8 * 16) + wib * kRing;
-    unsigned char* const stg0 = smem + kStepSmemHead + wib * 2 * G::BYTES;
-    if (lane == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar0 + 8, 1);
-        fence_mbar_init();
-    }
-    const int n = g.n_chunks;
-    const int W = (int)gridDim.x * wpb;
-    const int step = *g.cursor;
-    const int i0 = (int)blockIdx.x * wpb + wib;
-    // the records of this warp's chunks k = 0..31 (chunk i0 + k W), refilled every 32
-    {
-        const int i = i0 + lane * W;
-        if (i < n) ring[lane] = g.chunks[i];
-    }
-    __syncwarp();
-    uint32_t bytes_cur = i0 < n ? issue_chunk<DT, ODD, SINGLE>(g, ring[0], stg0, bar0, lane) : 0u, bytes_nxt = 0;
-    uint32_t parity = 0; // bit s: phase parity of stage s
-    int s = 0, k = 0;
-    bool ok = true;
-    for (int i = i0; i < n; i += W, ++k, s ^= 1) {
-        const int4 cur = ring[k & (kRing - 1)];
-        if (((k + 1) & (kRing - 1)) == 0) {
-            // refill the ring with the records of chunks k+1 .. k+32
-            __syncwarp();
-            const int j = i + (lane + 1) * W;
-            if (j < n) ring[lane] = g.chunks[j];
-            __syncwarp();
-        }
-        // stage the next chunk while this one computes
-        bytes_nxt = i + W < n ? issue_chunk<DT, ODD, SINGLE>(g, ring[(k + 1) & (kRing - 1)], stg0 + (s ^ 1) * G::BYTES,
-                                                             bar0 + 8 * (s ^ 1), lane)
-                              : 0u;
-        if (bytes_cur) {
-            ok = __all_sync(0xffffffffu, mbar_wait(bar0 + 8 * s, (parity >> s) & 1u));
-            if (!ok) {
-                // a staged chunk never arrived: flag it, let the copies in flight land, stop
-                if (lane == 0) atomicOr(SINGLE ? g.c0.err : g.cases[cur.z & CH_CASE_MASK].err, 2);
-                mbar_wait(bar0 + 8 * s, (parity >> s) & 1u);
-                if (bytes_nxt) mbar_wait(bar0 + 8 * (s ^ 1), (parity >> (s ^ 1)) & 1u);
-                break;
-            }
-            parity ^= 1u << s;
-        }
-        process_chunk<DT, COL, ODD, SINGLE>(g, cur, bytes_cur ? stg0 + s * G::BYTES : nullptr, step, lane);
-        // all reads of this stage are done before the next copy into it
-        fence_proxy_async_smem();
-        __syncwarp();
-        bytes_cur = bytes_nxt;
-    }
-    // the last block to finish advances the step cursor (every block has read it above)
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(g.done, 1) == (int)gridDim.x - 1) {
-            *g.done = 0;
-            *g.cursor = step + 1;
-            __threadfence();
-        }
+    using CT = typename Storage<DT>::CT;
+    const int lane = threadIdx.x & 31;
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int step = g.cursor[ODD ? 1 : 0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
+    // the step's flags are the same for every case of the group
+    const int flags = (SINGLE ? g.c0.ctl : g.cases[0].ctl)[step].flags;
+    if (w < g.n_chunks) {
+        const Chunk ch = g.chunks[w];
+        const int ci = ch.cflags & CH_CASE_MASK;
+        fluid_chunk<DT, COL, ODD>(SINGLE ? g.c0 : g.cases[ci], g.cases + ci, ch, flags, lane);
+    } else {
+        node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
     }
 }
 
@@ -637,7 +453,7 @@ __global__ void __launch_bounds__(128) k_bc_gather(const __grid_constant__ Group
     if (t >= g.n_gather) return;
     const int4 e = g.gather[t];
     const CaseArgs<CT>& a = g.cases[e.y];
-    const StepCtl<CT>& ctl = a.ctl[*g.cursor];
+    const StepCtl<CT>& ctl = a.ctl[g.cursor[ODD ? 1 : 0]];
     const int c = e.x, k = e.z;
     const int lab = a.label[c] & L_MASK;
     const int x = c % a.nx, y = (c / a.nx) % a.ny, z = c / (a.nx * a.ny);
@@ -688,12 +504,12 @@ __global__ void __launch_bounds__(256) k_refd_velocity(const __grid_constant__ G
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (warp >= g.n_chunks) return;
-    const int4 ch = g.chunks[warp];
-    const CaseArgs<CT>& a = g.cases[ch.z & CH_CASE_MASK];
+    const Chunk& ch = g.chunks[warp];
+    const CaseArgs<CT>& a = g.cases[ch.cflags & CH_CASE_MASK];
     if (a.cy_mode != CY_REF_FD) return;
-    const int y = ch.y & 0xffff, z = ch.y >> 16;
-    const int x = ch.x - y * a.nx - z * a.nx * a.ny + lane;
-    const int c = ch.x + lane;
+    const int y = ch.yz & 0xffff, z = ch.yz >> 16;
+    const int x = ch.c0 - y * a.nx - z * a.nx * a.ny + lane;
+    const int c = ch.c0 + lane;
     if (x >= a.nx || (a.label[c] & L_MASK) != L_FLUID) return;
     const int xs[3] = {x - 1, x, x + 1}, ys[3] = {y - 1, y, y + 1}, zs[3] = {z - 1, z, z + 1};
     CT f[27];
@@ -711,13 +527,13 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (warp >= g.n_chunks) return;
-    const int4 ch = g.chunks[warp];
-    const CaseArgs<CT>& a = g.cases[ch.z & CH_CASE_MASK];
+    const Chunk& ch = g.chunks[warp];
+    const CaseArgs<CT>& a = g.cases[ch.cflags & CH_CASE_MASK];
     if (a.cy_mode != CY_REF_FD) return;
     const int sy = a.nx, sz = a.nx * a.ny;
-    const int y = ch.y & 0xffff, z = ch.y >> 16;
-    const int x = ch.x - y * sy - z * sz + lane;
-    const int c = ch.x + lane;
+    const int y = ch.yz & 0xffff, z = ch.yz >> 16;
+    const int x = ch.c0 - y * sy - z * sz + lane;
+    const int c = ch.c0 + lane;
     if (x >= a.nx || (a.label[c] & L_MASK) != L_FLUID) return;
     CT* M = a.macro;
     const int64_t N = a.N;
@@ -747,35 +563,11 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
 // ---------------------------------------------------------------------------------------
 using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 
-// launch of one step-kernel variant: the dynamic shared memory is opted in once per
-// device, and the grid is capped at the blocks that are resident at once (persistent)
+// launch of one step-kernel variant: one warp per chunk
 template <int DT, int COL, bool ODD, bool SINGLE>
 void launch_step_variant(dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
-    auto kern = k_step<DT, COL, ODD, SINGLE>;
-    const int smem = step_smem_bytes<DT>((int)block.x / 32);
-    static std::atomic<unsigned long long> attr_set{0};
-    static std::atomic<int> resident[9] = {};  // per block size / 32
-    static std::atomic<int> sm_count{0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (!(attr_set.load() & bit)) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, step_smem_bytes<DT>(8));
-        attr_set.fetch_or(bit);
-    }
-    const int wpb = (int)block.x / 32;
-    if (wpb < 1 || wpb > 8) return;
-    if (!resident[wpb].load()) {
-        int nb = 0, sms = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, (int)block.x, smem);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        sm_count.store(std::max(sms, 1));
-        resident[wpb].store(std::max(nb, 1));
-    }
-    const unsigned cap = (unsigned)(resident[wpb].load() * sm_count.load());
-    const dim3 gr(std::max(1u, std::min(grid.x, cap)));
-    kern<<<gr, block, smem, s>>>(g);
+    k_step<DT, COL, ODD, SINGLE><<<grid, block, 0, s>>>(g);
 }
 
 template <int DT, int COL>

@@ -465,7 +465,10 @@ __device__ __forceinline__ CT cy_nu_from_central(CT Cxx, CT Cyy, CT Czz, CT Cxy,
 #pragma unroll
         for (int it = 0; it < 3; ++it) {
             const CT g = K / tau;
-            const CT s = dpow<CT>(p.lam * g, p.a);
+            // (lambda gamma)^a; in single precision the usual a = 2 is a product
+            CT s;
+            if constexpr (sizeof(CT) == 4) s = p.a == CT(2) ? (p.lam * g) * (p.lam * g) : dpow<CT>(p.lam * g, p.a);
+            else s = dpow<CT>(p.lam * g, p.a);
             const CT pw = dpow<CT>(CT(1) + s, e);
             const CT nuc = p.nu_inf + (p.nu0 - p.nu_inf) * pw;
             const CT G = tau - CT(3) * nuc - CT(0.5);
