@@ -9,7 +9,13 @@ step is preceded by a 512 MB buffer write that flushes L2, and steps are timed o
 with CUDA events on the library's stream.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
-                    [--dtype f32|f16|bf16|f64] [--collision CUM] [--no-stats]
+                    [--workload junction|dense_box] [--shape nx,ny,nz]
+                    [--dtype f32|f16|bf16|f64] [--collision CUM] [--no-stats] [--no-extras]
+
+On one GPU the FP32 line also carries, unless --no-extras, the same workload in FP16
+storage with the errors of FP32 and FP16 against FP64 on a short noisy-inflow run
+("storage_f16"), and, for the junction, the 15-case study batched in one launch group
+against the cases stepped one after another ("batch").
 
 Multi-GPU (launched by torchrun, one rank per GPU): every rank runs its own replica of the
 case (the path has no exchange step on one GPU); value = all fluid-cell updates / max time.
@@ -49,6 +55,7 @@ def parse():
     ap.add_argument("--no-stats", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=400)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP16-storage and 15-case batch measurements")
     return ap.parse_args()
 
 
@@ -276,10 +283,78 @@ def main() -> int:
         dist.close()
 
 
+class L2Flush:
+    """Every timed step starts from a cold L2: a 512 MB write, then a 256 MB read that leaves
+    L2 holding clean lines (so the flush's own write-back does not land in the step)."""
+
+    def __init__(self, dev: int):
+        import torch
+
+        self.flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{dev}")
+        self.clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{dev}")
+        self.sink = torch.zeros(1, dtype=torch.int64, device=f"cuda:{dev}")
+
+    def __call__(self):
+        self.flush.zero_()
+        self.sink += self.clean.sum()
+
+
+def timed_steps(lat, steps: int, stats: bool, flush: L2Flush, dev: int) -> float:
+    """Device milliseconds of `steps` single steps, each bracketed by CUDA events on the
+    library's stream after an L2 flush outside the events; the steps are enqueued without
+    host waits (NNLBM_STEP_ASYNC) and the watchdog is checked once at the end."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush()
+            ev[k][0].record(stream)
+            lat.step(1, stats=stats, wait=False)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    lat.sync()
+    return sum(e0.elapsed_time(e1) for e0, e1 in ev)
+
+
+def storage_comparison(a, flush: L2Flush, dev: int, f32_mlups: float) -> dict:
+    """FP16 storage on the same workload and timing, beside the FP32 line, with the error of
+    a short FP16 and FP32 run of the junction against FP64 (studies.precision_study)."""
+    from nonnewlbm_b200 import studies
+    from nonnewlbm_b200 import workloads as W
+
+    w = workload(a, "f16")
+    lat = W.build_lattice(w, device=dev)
+    fluid = lat.step_info()["fluid_cells"]
+    lat.autotune()
+    lat.step(max(3, a.warmup), stats=not a.no_stats)
+    n = max(20, min(a.steps, 200))
+    ms = timed_steps(lat, n, not a.no_stats, flush, dev)
+    lat.close()
+    f16 = fluid * n / (ms / 1e3) / 1e6
+    err = studies.precision_study(scale=1.0, steps=2000, collision=a.collision, dtypes=("f64", "f32", "f16"), device=dev)
+    r = err["runs"]
+    return {"f16_mlups": round(f16, 2), "f32_mlups": round(f32_mlups, 2), "ratio_f16_f32": round(f16 / f32_mlups, 3),
+            "error_vs_f64": {k: {e: r[k][e] for e in ("velocity_l2_rel", "velocity_linf_rel", "outlet_split_abs_err",
+                                                       "wss_l2_rel")} for k in ("f32", "f16")},
+            "error_run": f"{err['workload']} {err['collision']} local-neq CY, 2000 steps, inflow noise +-5 %/100 steps, "
+                         f"seed {err['seed']}"}
+
+
+def batch_gain(dev: int) -> dict:
+    """The 15-case study (5 inflow pairs x 3 rheologies, seeded scales in [0.5, 1]): one
+    batched launch group against the cases stepped one after another."""
+    from nonnewlbm_b200 import studies
+
+    r = studies.run_batch(studies.batch_cases(seed=2024, dtype="f32"), steps=100, warmup=10, device=dev)
+    return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items() if k != "scales"}
+
+
 def run_ours(a, dist: Dist) -> int:
     import torch
 
-    from nonnewlbm_b200 import capi
     from nonnewlbm_b200 import workloads as W
 
     dev = dist.local
@@ -289,33 +364,17 @@ def run_ours(a, dist: Dist) -> int:
     lat = W.build_lattice(w, device=dev)
     info = lat.step_info()
     lat.autotune()
-    stream = torch.cuda.ExternalStream(lat.stream, device=dev)
     lat.step(max(3, a.warmup), stats=stats)
     # the populations touched per step can be smaller than the 126 MB L2 (a sparse
-    # junction): every timed step starts from a cold L2 by writing a 512 MB buffer first,
-    # outside the step's events
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{dev}")
-    # a read of a second buffer after the write leaves L2 holding clean lines, so the
-    # write-back of the flush does not land inside the timed step
-    clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.int32, device=f"cuda:{dev}")
-    sink = torch.zeros(1, dtype=torch.int64, device=f"cuda:{dev}")
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    # junction), so every timed step starts from a cold L2
+    flush = L2Flush(dev)
     sampler = ClockSampler(dev)
     sampler.start()
     time.sleep(0.3)
     dist.barrier()
-    torch.cuda.synchronize(dev)
-    with torch.cuda.stream(stream):
-        for k in range(a.steps):
-            flush.zero_()
-            sink += clean.sum()
-            ev[k][0].record(stream)
-            lat.step(1, stats=stats)
-            ev[k][1].record(stream)
-    torch.cuda.synchronize(dev)
+    ms = timed_steps(lat, a.steps, stats, flush, dev)
     dist.barrier()
     clocks = sampler.stop()
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in ev)
     ms = dist.max(ms)
     fluid = info["fluid_cells"]
     value = fluid * a.steps * dist.world / (ms / 1e3) / 1e6
@@ -330,7 +389,7 @@ def run_ours(a, dist: Dist) -> int:
     traffic = ncu_traffic(key)
 
     # end to end through the public API: per step the host sends that step's inflow row
-    # (pinned staging inside the library) and reads back the FP64 mass / flux sums
+    # and reads back the FP64 mass / flux sums
     if w.kind == "tcpc":
         rows = np.array([[w.u_ivc * w.notes["counts"]["left_area"], w.u_svc * w.notes["counts"]["right_area"], 1.0]])
     else:
@@ -348,6 +407,7 @@ def run_ours(a, dist: Dist) -> int:
     ctl_bytes = 32 if w.dtype != "f64" else 56
     h2d = ctl_bytes + 8  # the step's control row + the cursor reset
     d2h = 5 * 8 + 3 * 4  # mass/flux sums + the watchdog / cursor words
+    lat.close()
 
     if dist.rank == 0:
         line = {
@@ -370,9 +430,12 @@ def run_ours(a, dist: Dist) -> int:
         }
         if dist.world == 1:
             line["cpu_baseline"] = cpu_baseline_sample(w, a.cpu_seconds, a.collision)
+            if not a.no_extras and a.dtype == "f32":
+                line["storage_f16"] = storage_comparison(a, flush, dev, value)
+                if a.workload == "junction":
+                    line["batch"] = batch_gain(dev)
         line["reduce_last"] = [float(v) for v in red] if red is not None else None
         print(json.dumps(line))
-    lat.close()
     return 0
 
 

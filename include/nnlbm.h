@@ -88,7 +88,9 @@ enum {
 enum {
     NNLBM_STEP_STATS = 1, /* accumulate the mean/rms sums (MacroTcpc::outputMacro, sim_tcpc.cu:347-353) */
     NNLBM_STEP_MACRO = 2, /* store rho, u, F and S of every cell */
-    NNLBM_STEP_REDUCE = 4 /* FP64 mass and plane-flux sums (nnlbm_reduce) */
+    NNLBM_STEP_REDUCE = 4, /* FP64 mass and plane-flux sums (nnlbm_reduce) */
+    NNLBM_STEP_ASYNC = 8   /* enqueue the steps and return without waiting; the watchdog is
+                              checked by the next nnlbm_sync or synchronous nnlbm_step */
 };
 
 /* One lattice (case).  Physical inputs are already in lattice units; the unit conversions
@@ -224,6 +226,12 @@ int nnlbm_step_info(nnlbm_ctx* ctx, int ic, int64_t* fluid_cells, int64_t* bc_ce
  * in launches[5].  The steps are real steps (the lattice advances).  No reference
  * counterpart (the reference logs wall-clock MLUPS, core.h:1440-1469). */
 int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, double* ms, int64_t* launches);
+
+/* Wait for every step enqueued on the context's stream and check the watchdog: returns
+ * NNLBM_ERR_NAN if a density left (0.25, 4) or became non-finite.  The reference's step
+ * loop synchronises the device after every SimUpdate (core.h:1197-1198, 1256-1257); with
+ * NNLBM_STEP_ASYNC the caller chooses when. */
+int nnlbm_sync(nnlbm_ctx* ctx);
 
 /* Raw CUDA stream (cudaStream_t) of the context, for callers that interleave their own work. */
 void* nnlbm_stream(nnlbm_ctx* ctx);

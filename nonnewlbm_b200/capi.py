@@ -21,14 +21,14 @@ EQ_INV_CUM_REF, EQ_INV_CUM, EQ_DEFAULT, EQ_ENTROPIC = 0, 1, 2, 3
 EQUILIBRIA = {"inv_cum_ref": 0, "inv_cum": 1, "default": 2, "entropic": 3}
 CY_NONE, CY_REF_FD, CY_LOCAL_NEQ = 0, 1, 2
 CY_MODES = {"none": 0, "ref-fd": 1, "ref_fd": 1, "local-neq": 2, "local_neq": 2}
-STEP_STATS, STEP_MACRO, STEP_REDUCE = 1, 2, 4
+STEP_STATS, STEP_MACRO, STEP_REDUCE, STEP_ASYNC = 1, 2, 4, 8
 M_RHO, M_VX, M_VY, M_VZ, M_FX, M_FY, M_FZ, M_S11, M_S12, M_S13, M_S22, M_S32, M_S33 = range(13)
 
 EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
     "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_step_noalloc", "nnlbm_stat_reset", "nnlbm_get_macro",
     "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_step_info", "nnlbm_profile_step",
-    "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels",
+    "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels", "nnlbm_sync",
 ]
 
 
@@ -81,6 +81,7 @@ def lib():
         L.nnlbm_autotune.argtypes = [_vp]
         L.nnlbm_step_info.argtypes = [_vp, i, _i64p, _i64p, _i64p, _dp]
         L.nnlbm_profile_step.argtypes = [_vp, i, ctypes.c_int64, i, _dp, _i64p]
+        L.nnlbm_sync.argtypes = [_vp]
         L.nnlbm_stream.argtypes = [_vp]
         L.nnlbm_stream.restype = _vp
         L.nnlbm_last_error.argtypes = [_vp, ctypes.c_char_p, ctypes.c_size_t]

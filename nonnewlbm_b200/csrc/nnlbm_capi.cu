@@ -107,6 +107,7 @@ struct Case {
     int64_t n_fluid = 0, n_bc = 0, left_area = 0, right_area = 0, n_inflow_eq = 0;
     double ivc_flux = 0, svc_flux = 0, rho_left = 1, rho_right = 1, rho_eq = 1;
     std::vector<double> sched;       // rows of {ivc_flux, svc_flux, profile_scale}
+    mutable std::vector<char> ctl_dev; // copy of the leading control rows on the device (empty: unknown)
     int64_t parity = 0;              // steps done since the layout was last reset, mod 2
     int64_t iterations = 0;
     int64_t n_stats = 0;
@@ -228,6 +229,7 @@ int ensure_stats(nnlbm_ctx* ctx, Case& c)
 int ensure_ctl(nnlbm_ctx* ctx, Case& c, int64_t n)
 {
     if (c.ctl_cap >= n && c.d_ctl) return NNLBM_OK;
+    c.ctl_dev.clear();
     int64_t cap = std::max<int64_t>(n, 1024);
     if (c.d_ctl) cudaFree(c.d_ctl);
     c.d_ctl = nullptr;
@@ -282,7 +284,8 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
             ch.cflags = (int)j | (ch.cflags & ~CH_CASE_MASK);
             chunks.push_back(ch);
         }
-        for (int32_t k : c.gather_self) gather.push_back(make_int4(c.self_cell[k], (int)j, (int)(self_off + k), 0));
+        for (int32_t k : c.gather_self)
+            gather.push_back(make_int4(c.self_cell[k], (int)j, (int)(self_off + k), (int)c.label[c.self_cell[k]]));
         for (int32_t cell : c.self_cell) nodes.push_back(make_int2(cell, (int)j));
         for (double v : c.self_prof) prof.push_back((CT)v);
         self_off += (int64_t)c.self_cell.size();
@@ -348,7 +351,7 @@ int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
         A.refd_velocity(odd, cgrid, cblk, ctx->stream, g.args.data());
         A.refd_stress(odd, cgrid, cblk, ctx->stream, g.args.data());
     }
-    if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 127) / 128), dim3(128), ctx->stream, g.args.data());
+    if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
     step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, g.args.data());
     CK(cudaGetLastError());
     return NNLBM_OK;
@@ -393,7 +396,11 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags)
         std::vector<char> buf;
         if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n, flags);
         else fill_ctl<float>(c, buf, n, flags);
-        CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
+        // rows already on the device (a constant inflow stepped call after call) are not sent again
+        if (buf.size() > c.ctl_dev.size() || memcmp(buf.data(), c.ctl_dev.data(), buf.size()) != 0) {
+            CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
+            c.ctl_dev = buf;
+        }
         if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
     }
     if ((rc = prepare_group(ctx, g)) != NNLBM_OK) return rc;
@@ -540,7 +547,8 @@ int upload_ctl_rows(nnlbm_ctx* ctx, const Case& c, int64_t n, int flags)
             r[j].rho_left = (CT)c.rho_left; r[j].rho_right = (CT)c.rho_right; r[j].rho_eq = (CT)c.rho_eq;
             r[j].prof_scale = (CT)ps;
         }
-        // pageable source: the call returns once the rows have been staged, so r is reusable
+        c.ctl_dev.clear();
+    // pageable source: the call returns once the rows have been staged, so r is reusable
         CK(cudaMemcpyAsync((StepCtl<CT>*)c.d_ctl + k0, r, cnt * sizeof(StepCtl<CT>), cudaMemcpyHostToDevice, ctx->stream));
     }
     return NNLBM_OK;
@@ -869,7 +877,21 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         if (n_steps < rows) c.sched.erase(c.sched.begin(), c.sched.begin() + 3 * n_steps);
         else c.sched.erase(c.sched.begin(), c.sched.end() - 3);
     }
+    if (flags & NNLBM_STEP_ASYNC) return NNLBM_OK;
     return wait_and_check(ctx, n_steps);
+}
+
+int nnlbm_sync(nnlbm_ctx* ctx)
+{
+    if (!ctx) return NNLBM_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<int> err(ctx->cases.size());
+    for (size_t i = 0; i < ctx->cases.size(); ++i)
+        CK(cudaMemcpyAsync(&err[i], ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < ctx->cases.size(); ++i)
+        if (err[i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
+    return NNLBM_OK;
 }
 
 int nnlbm_stat_reset(nnlbm_ctx* ctx, int ic)
@@ -1099,7 +1121,7 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
             mark(4);
         }
         if (g.n_gather > 0) {
-            A.gather(odd, dim3((g.n_gather + 127) / 128), dim3(128), ctx->stream, g.args.data());
+            A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
             mark(0);
         }
         step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, g.args.data());
@@ -1187,7 +1209,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
                 A.refd_velocity(odd, cgrid, cblk, ctx->stream, args);
                 A.refd_stress(odd, cgrid, cblk, ctx->stream, args);
             }
-            if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 127) / 128), dim3(128), ctx->stream, args);
+            if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, args);
             step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, args);
         }
         CK(cudaGetLastError());

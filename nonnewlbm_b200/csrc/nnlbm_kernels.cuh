@@ -128,7 +128,7 @@ struct GroupArgs {
     const CaseArgs<CT>* cases;
     const Chunk* chunks;
     int n_chunks, pad0;
-    const int4* gather;        // {cell, case, node index, 0} of the open-plane nodes
+    const int4* gather;        // {cell, case, node index, label} of the open-plane nodes
     int n_gather, n_nodes;
     const int2* nodes;         // [n_nodes] {cell, case} of every boundary node (open planes, INFLOW_EQ)
     const CT* bc_prof;         // [n_nodes][3] prescribed velocity (GEO_INFLOW nodes)
@@ -446,16 +446,17 @@ __device__ __forceinline__ void pull_triples(const CaseArgs<typename Storage<DT>
 }
 
 template <int DT, bool ODD>
-__global__ void __launch_bounds__(128) k_bc_gather(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
+__global__ void __launch_bounds__(64) k_bc_gather(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.n_gather) return;
+    // {cell, case, node index, label}: the stencil loads depend on nothing but this record
     const int4 e = g.gather[t];
     const CaseArgs<CT>& a = g.cases[e.y];
     const StepCtl<CT>& ctl = a.ctl[g.cursor[ODD ? 1 : 0]];
     const int c = e.x, k = e.z;
-    const int lab = a.label[c] & L_MASK;
+    const int lab = e.w;
     const int x = c % a.nx, y = (c / a.nx) % a.ny, z = c / (a.nx * a.ny);
     // clamped neighbours of a non-periodic cell (core.h:651-661)
     const int xm = max(x - 1, 0), xp = min(x + 1, a.nx - 1), ym = max(y - 1, 0), yp = min(y + 1, a.ny - 1);

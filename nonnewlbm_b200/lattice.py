@@ -115,9 +115,16 @@ class Lattice:
         self._chk(capi.lib().nnlbm_set_schedule(self.h, ic, capi.dptr(a), a.shape[0]))
 
     # -- time stepping --------------------------------------------------------------------
-    def step(self, n: int = 1, stats: bool = False, macro: bool = False, reduce: bool = False) -> None:
+    def step(self, n: int = 1, stats: bool = False, macro: bool = False, reduce: bool = False, wait: bool = True) -> None:
+        """Advance n steps.  wait=False enqueues them and returns at once (NNLBM_STEP_ASYNC);
+        sync() then waits and checks the watchdog."""
         flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0) | (capi.STEP_REDUCE if reduce else 0)
+        if not wait:
+            flags |= capi.STEP_ASYNC
         self._chk(capi.lib().nnlbm_step(self.h, int(n), flags))
+
+    def sync(self) -> None:
+        self._chk(capi.lib().nnlbm_sync(self.h))
 
     def step_noalloc(self, n: int = 1, stats: bool = False, macro: bool = False, reduce: bool = False) -> None:
         """nnlbm_step_noalloc: the same steps without any device allocation (the buffers the

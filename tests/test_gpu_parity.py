@@ -241,3 +241,29 @@ def test_batched_mixed_groups_and_sizes():
     for k in range(3):
         assert np.array_equal(lat.export_df(k), singles[k].export_df())
         assert np.array_equal(lat.stats(k)[0], singles[k].stats()[0])
+
+
+def test_async_steps_and_control_rows_match_sync():
+    """Steps enqueued without waiting (NNLBM_STEP_ASYNC, then nnlbm_sync) and one-step calls
+    whose unchanged control rows are not sent again give the same lattice as synchronous
+    multi-step calls; a changed inflow between calls takes effect."""
+    wall = small_junction()
+    nz, ny, nx = wall.shape
+    lats = [Lattice(CaseSpec((nx, ny, nz), collision="CUM", dtype="f64", nu=0.02)) for _ in range(2)]
+    for L in lats:
+        c = L.setup_tcpc(wall)
+        L.set_inflow(ivc_flux=0.03 * c["left_area"], svc_flux=0.02 * c["right_area"])
+        L.init_equilibrium()
+    a, b = lats
+    a.step(6, stats=True)
+    for _ in range(6):
+        b.step(1, stats=True, wait=False)
+    b.sync()
+    for L in lats:
+        L.set_inflow(ivc_flux=40.0, svc_flux=10.0)
+    a.step(5)
+    for _ in range(5):
+        b.step(1, wait=False)
+    b.sync()
+    assert np.array_equal(a.export_df(), b.export_df())
+    assert np.array_equal(a.stats()[0], b.stats()[0])
