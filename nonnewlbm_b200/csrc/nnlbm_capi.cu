@@ -338,8 +338,13 @@ int prepare_group(nnlbm_ctx* ctx, Group& g)
     return g.dtype == NNLBM_F64 ? upload_group<double>(ctx, g) : upload_group<float>(ctx, g);
 }
 
-// warps of one step launch: one per chunk, then one per 32 boundary nodes
-int step_warps(const Group& g) { return std::max(g.n_chunks + (int)((g.n_self + 31) / 32), 1); }
+// warps of one step launch: one per chunk (per two chunks where the step pairs them),
+// then one per 32 boundary nodes
+int step_warps(const Group& g)
+{
+    const int cw = pairs_chunks(g.dtype, g.collision) ? (g.n_chunks + 1) / 2 : g.n_chunks;
+    return std::max(cw + (int)((g.n_self + 31) / 32), 1);
+}
 
 // enqueue one step of a group (no host synchronisation); `odd` is the A-A parity
 int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
@@ -347,9 +352,10 @@ int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
     const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
+    const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
     if (g.any_refd) {
-        A.refd_velocity(odd, cgrid, cblk, ctx->stream, g.args.data());
-        A.refd_stress(odd, cgrid, cblk, ctx->stream, g.args.data());
+        A.refd_velocity(odd, rgrid, cblk, ctx->stream, g.args.data());
+        A.refd_stress(odd, rgrid, cblk, ctx->stream, g.args.data());
     }
     if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
     step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, g.args.data());
@@ -1099,6 +1105,7 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
     const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
+    const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
     for (int i = 0; i < 5; ++i) { ms[i] = 0; launches[i] = 0; }
     const int64_t parity = ctx->cases[g.cases[0]].parity;
     // kinds: 0 gather, 1 step, 3 CY_REF_FD velocity, 4 CY_REF_FD strain
@@ -1115,9 +1122,9 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
         const bool odd = ((parity + k) & 1) != 0;
         if (mark(-1)) return set_err(ctx, NNLBM_ERR_CUDA, "event record failed");
         if (g.any_refd) {
-            A.refd_velocity(odd, cgrid, cblk, ctx->stream, g.args.data());
+            A.refd_velocity(odd, rgrid, cblk, ctx->stream, g.args.data());
             mark(3);
-            A.refd_stress(odd, cgrid, cblk, ctx->stream, g.args.data());
+            A.refd_stress(odd, rgrid, cblk, ctx->stream, g.args.data());
             mark(4);
         }
         if (g.n_gather > 0) {
@@ -1202,12 +1209,13 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         const AuxLaunchers& A = aux_launchers(g.dtype);
         const int per_block = g.block / kChunk;
         const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
+        const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
         const int64_t parity = ctx->cases[g.cases[0]].parity;
         for (int64_t k = 0; k < n_steps; ++k) {
             const bool odd = ((parity + k) & 1) != 0;
             if (g.any_refd) {
-                A.refd_velocity(odd, cgrid, cblk, ctx->stream, args);
-                A.refd_stress(odd, cgrid, cblk, ctx->stream, args);
+                A.refd_velocity(odd, rgrid, cblk, ctx->stream, args);
+                A.refd_stress(odd, rgrid, cblk, ctx->stream, args);
             }
             if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, args);
             step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, args);

@@ -14,18 +14,18 @@
 // solver/sim_tcpc/sim_tcpc.cu:235-241) need no work at all under A-A: their post-step
 // value f*_q = incoming f_opp(q) already sits in the slot the neighbour reads next.
 //
-// Work decomposition: a packed list of 32-cell row chunks (one warp each) that contain a
-// cell with work, over all cases of a launch group (same storage type and collision).
-// Per-case parameters live in a device array indexed by the chunk's case.
+// Work decomposition: a packed list of 32-cell row chunks of colliding cells (one warp
+// each, or one warp per two chunks for the single-precision cumulant), over all cases of
+// a launch group (same storage type and collision), followed by warps of 32 boundary
+// nodes.  Per-case parameters live in a device array indexed by the chunk's case (and in
+// parameter space for a single-case group).
 //
 // Open-plane nodes (TCPC IVC/SVC inflow and outlets, generic GEO_OUTFLOW_RIGHT_EQ) pull a
-// stencil re-centred one cell inward (sim_tcpc.cu:242-273, lbm_bc.h:147-152).  Those
-// populations are exactly the ones the inward neighbour pulls for itself, so when that
-// neighbour is a FLUID/PERIODIC cell with the same tangential stencil ("source") its own
-// thread computes the node's density / velocity and writes the node's equilibrium into
-// the node's slots (which no other cell touches within the step).  The remaining nodes
-// (corners, CY_REF_FD outlets) are gathered by k_bc_gather before the step kernel and
-// written by their own thread; GEO_INFLOW nodes need no gather at all.
+// stencil re-centred one cell inward (sim_tcpc.cu:242-273, lbm_bc.h:147-152).  k_bc_gather
+// computes their density / velocity from the pre-step state before the step kernel runs;
+// the node warps of the step kernel then write each node's equilibrium into the node's
+// own slots, which no other cell touches within the step.  GEO_INFLOW nodes take their
+// prescribed velocity and need no gather.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -267,14 +267,15 @@ __device__ __noinline__ void refd_force(const CaseArgs<CT>* ap, int c, int sy, i
     F[2] += CT(2) * (nuc - a.nu) * F3;
 }
 
-// minimum resident blocks of 256 threads: the register budget of each variant (FP64
-// arithmetic and the KBC family need more live values than the cumulant in FP32)
-#ifndef NNLBM_STEP_MINB
-#define NNLBM_STEP_MINB 2
+// register budget per thread of each step-kernel variant: FP64 arithmetic may use all
+// 255; the paired cumulant (two cells per thread) gets NNLBM_PAIR_REGS; everything else
+// 128, two 256-thread blocks per SM
+#ifndef NNLBM_PAIR_REGS
+#define NNLBM_PAIR_REGS 128
 #endif
 template <int DT, int COL>
-struct StepOccupancy {
-    static constexpr int value = DT == 0 ? 1 : ((COL >= COL_KBC_N1 && COL <= COL_KBC_C4) ? 2 : NNLBM_STEP_MINB);
+struct StepRegs {
+    static constexpr int value = DT == 0 ? 255 : COL == COL_CUM ? NNLBM_PAIR_REGS : 128;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -287,7 +288,7 @@ struct StepOccupancy {
 // ---------------------------------------------------------------------------------------
 template <int DT, int COL, bool ODD>
 __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>::CT>& a, const CaseArgs<typename Storage<DT>::CT>* ap,
-                                            const Chunk& ch, int flags, int lane)
+                                            const Chunk& ch, int step, int flags, int lane)
 {
     using S = Storage<DT>;
     using T = typename S::T;
@@ -363,6 +364,88 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// two plain chunks of one case in one warp, one cell of each per lane, for the cumulant
+// in single-precision arithmetic: the two cells' arithmetic runs as f2 on the packed
+// FP32 pipe, so the pair issues about the FP32 instructions of one cell; loads, stores
+// and the per-cell outputs stay per cell.  A lane whose cell in one chunk does not
+// collide computes that half from the rest state and stores nothing for it.
+// ---------------------------------------------------------------------------------------
+template <int DT> struct Raw;
+template <> struct Raw<1> { __device__ static __forceinline__ float get(float v) { return v; } };
+template <> struct Raw<2> { __device__ static __forceinline__ float get(__half v) { return __half2float(v); } };
+template <> struct Raw<3> { __device__ static __forceinline__ float get(__nv_bfloat16 v) { return __bfloat162float(v); } };
+template <int DT> struct Cook;
+template <> struct Cook<1> { __device__ static __forceinline__ float put(float v) { return v; } };
+template <> struct Cook<2> { __device__ static __forceinline__ __half put(float v) { return __float2half_rn(v); } };
+template <> struct Cook<3> { __device__ static __forceinline__ __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); } };
+
+template <int DT, bool ODD>
+__device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseArgs<float>* ap, const Chunk& ca, const Chunk& cb,
+                                           int step, int flags, int lane)
+{
+    using T = typename Storage<DT>::T;
+    const unsigned bit = 1u << lane;
+    const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
+    double mass = 0.0;
+    if (fa || fb) {
+        const int cA = ca.c0 + lane, cB = cb.c0 + lane;
+        const int64_t qs = a.qstride, sy = a.nx, sz = (int64_t)a.nx * a.ny;
+        const T* pa = (const T*)a.df + cA;
+        const T* pb = (const T*)a.df + cB;
+        const f2 isc(a.inv_scale);
+        f2 f[27];
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const int64_t o = ODD ? oppq(q) * qs - (cxq(q) + cyq(q) * sy + czq(q) * sz) : q * qs;
+            const f2 raw(fa ? Raw<DT>::get(pa[o]) : 0.f, fb ? Raw<DT>::get(pb[o]) : 0.f);
+            const f2 w(weight<float>(q));
+            f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
+        }
+        f2 rho, ux, uy, uz;
+        density_velocity<f2>(f, f2(a.fx), f2(a.fy), f2(a.fz), rho, ux, uy, uz);
+        f2 Sl[6];
+        const CYParams<float> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
+        collide_cum<f2, float>(f, rho, ux, uy, uz, f2(a.nu), a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
+        T* qa = (T*)a.df + cA;
+        T* qb = (T*)a.df + cB;
+        const f2 sc(a.scale);
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const int64_t o = ODD ? q * qs + (cxq(q) + cyq(q) * sy + czq(q) * sz) : oppq(q) * qs;
+            const f2 w(weight<float>(q));
+            const f2 v = DT == 1 ? f[q] - w : (f[q] - w) * sc;
+            if (fa) qa[o] = Cook<DT>::put(v.v.x);
+            if (fb) qb[o] = Cook<DT>::put(v.v.y);
+        }
+        const float r[2] = {rho.v.x, rho.v.y}, u0[2] = {ux.v.x, ux.v.y}, u1[2] = {uy.v.x, uy.v.y}, u2[2] = {uz.v.x, uz.v.y};
+        const bool on[2] = {fa, fb};
+        const int cc[2] = {cA, cB};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (!on[h]) continue;
+            if (flags & F_MACRO) {
+                write_macro<float>(a, cc[h], r[h], u0[h], u1[h], u2[h], a.fx, a.fy, a.fz);
+                if (a.cy_mode == CY_LOCAL_NEQ) {
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) a.macro[(int64_t)(M_S11 + k) * a.N + cc[h]] = h ? Sl[k].v.y : Sl[k].v.x;
+                }
+            }
+            if (flags & F_STATS) accumulate_stats<float>(a, cc[h], r[h], u0[h], u1[h], u2[h]);
+            if (!(r[h] > 0.25f && r[h] < 4.f)) atomicOr(a.err, 1);
+            mass += (double)r[h];
+        }
+    }
+    if (flags & F_REDUCE) {
+        const double s0 = warp_sum(mass);
+        if (lane == 0 && s0 != 0.0) atomicAdd(a.red, s0);
+    }
+}
+
+// the step kernel of a (storage, collision) pairs its plain chunks (fluid_pair) when the
+// arithmetic is single precision and the collision is the cumulant
+__host__ __device__ constexpr bool pairs_chunks(int dt, int col) { return dt != 0 && col == COL_CUM; }
+
 // 32 boundary nodes (open-plane nodes and GEO_INFLOW nodes, one per lane): each writes
 // the equilibrium of its gathered (rho, u) (or of its prescribed inflow) into its own
 // slots, which no other cell reads or writes within the step, and adds its plane flux
@@ -399,7 +482,7 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
 // the step kernel: one warp per chunk of the work list, then one warp per 32 boundary
 // nodes.  Both write only the slots their own cells read, so they run side by side.
 template <int DT, int COL, bool ODD, bool SINGLE>
-__global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
+__global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
     k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
@@ -409,17 +492,42 @@ __global__ void __launch_bounds__(256, StepOccupancy<DT, COL>::value)
     if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
     // the step's flags are the same for every case of the group
     const int flags = (SINGLE ? g.c0.ctl : g.cases[0].ctl)[step].flags;
-    if (w < g.n_chunks) {
-        const Chunk ch = g.chunks[w];
-        const int ci = ch.cflags & CH_CASE_MASK;
-        fluid_chunk<DT, COL, ODD>(SINGLE ? g.c0 : g.cases[ci], g.cases + ci, ch, flags, lane);
+    if constexpr (pairs_chunks(DT, COL)) {
+        // warp w takes chunks 2w and 2w + 1; a pair that is not two plain chunks of one case
+        // (without the finite-difference force) is stepped chunk by chunk
+        const int np = (g.n_chunks + 1) >> 1;
+        if (w < np) {
+            const Chunk ca = g.chunks[2 * w];
+            Chunk cb{};
+            if (2 * w + 1 < g.n_chunks) cb = g.chunks[2 * w + 1];
+            else cb.cflags = ca.cflags; // empty partner: no colliding lane
+            const int ci = ca.cflags & CH_CASE_MASK;
+            const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[ci];
+            if (((ca.cflags & cb.cflags) & CH_PLAIN) && ci == (cb.cflags & CH_CASE_MASK) && a.cy_mode != CY_REF_FD) {
+                fluid_pair<DT, ODD>(a, g.cases + ci, ca, cb, step, flags, lane);
+            } else {
+                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, step, flags, lane);
+                if (cb.fluid) {
+                    const int cj = cb.cflags & CH_CASE_MASK;
+                    fluid_chunk<DT, COL, ODD>(SINGLE ? g.c0 : g.cases[cj], g.cases + cj, cb, step, flags, lane);
+                }
+            }
+        } else {
+            node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - np) * 32 + lane, step, flags);
+        }
     } else {
-        node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
+        if (w < g.n_chunks) {
+            const Chunk ch = g.chunks[w];
+            const int ci = ch.cflags & CH_CASE_MASK;
+            fluid_chunk<DT, COL, ODD>(SINGLE ? g.c0 : g.cases[ci], g.cases + ci, ch, step, flags, lane);
+        } else {
+            node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
+        }
     }
 }
 
 // ---------------------------------------------------------------------------------------
-// gathered open-plane nodes (the ones without a source neighbour)
+// open-plane nodes: the re-centred stencil of each, before the step
 // ---------------------------------------------------------------------------------------
 // canonical post-collision population q of cell (x,y,z) of the previous step, in the A-A
 // layout that step left behind

@@ -36,6 +36,34 @@ template <> __device__ __forceinline__ float dpow<float>(float b, float e) { ret
 template <> __device__ __forceinline__ double dpow<double>(double b, double e) { return pow(b, e); }
 
 // ---------------------------------------------------------------------------------------
+// f2: one quantity of two cells at once on the packed FP32 pipe of sm_100 (FADD2, FMUL2,
+// FFMA2), so that the step of two cells issues the arithmetic instructions of one.  Each
+// half is rounded exactly as the scalar float operation; division is per half.
+// ---------------------------------------------------------------------------------------
+struct f2 {
+    float2 v;
+    __device__ __forceinline__ f2() {}
+    __device__ __forceinline__ f2(float2 a) : v(a) {}
+    __device__ __forceinline__ f2(float a, float b) : v(make_float2(a, b)) {}
+    __device__ __forceinline__ explicit f2(double s) : v(make_float2((float)s, (float)s)) {}
+};
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) { return __fadd2_rn(a.v, b.v); }
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) { return __fmul2_rn(a.v, b.v); }
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) { return __ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v); }
+__device__ __forceinline__ f2 operator-(f2 a) { return __fmul2_rn(a.v, make_float2(-1.f, -1.f)); }
+__device__ __forceinline__ f2 operator/(f2 a, f2 b) { return f2(a.v.x / b.v.x, a.v.y / b.v.y); }
+__device__ __forceinline__ f2& operator+=(f2& a, f2 b) { return a = a + b; }
+__device__ __forceinline__ f2& operator-=(f2& a, f2 b) { return a = a - b; }
+
+// a b + c: one rounding for f2 (FFMA2); for float the compiler contracts it under
+// --use_fast_math; for double (built with -fmad=false) it is the product, then the sum,
+// so an expression rewritten with mad keeps its FP64 rounding
+template <class CT>
+__device__ __forceinline__ CT mad(CT a, CT b, CT c) { return a * b + c; }
+template <>
+__device__ __forceinline__ f2 mad<f2>(f2 a, f2 b, f2 c) { return __ffma2_rn(a.v, b.v, c.v); }
+
+// ---------------------------------------------------------------------------------------
 // density and velocity with the F/2 shift, in the pairwise order of Geier 2015 Appendix J
 // (the order of LBM_COMMON::computeDensityAndVelocity, solver/lbm3d/lbm_common.h:31-38)
 // ---------------------------------------------------------------------------------------
@@ -137,17 +165,22 @@ __device__ void equilibrium(int eq, CT rho, CT ux, CT uy, CT uz, CT* f)
 template <class CT>
 __device__ __forceinline__ void fwd3(CT m, CT z, CT p, CT u, CT& k0, CT& k1, CT& k2)
 {
-    k0 = (p + m) + z;
-    k1 = (p - m) - u * k0;
-    k2 = (p + m) - CT(2) * u * (p - m) + u * u * k0;
+    // k0 = (p+m)+z, k1 = (p-m) - u k0, k2 = (p+m) - 2u (p-m) + u^2 k0
+    const CT s = p + m, d = p - m;
+    k0 = s + z;
+    k1 = mad(-u, k0, d);
+    k2 = mad(u * u, k0, mad(-(CT(2) * u), d, s));
 }
 
 template <class CT>
 __device__ __forceinline__ void bwd3(CT k0, CT k1, CT k2, CT u, CT& m, CT& z, CT& p)
 {
-    z = k0 * (CT(1) - u * u) - CT(2) * u * k1 - k2;
-    m = (k0 * (u * u - u) + k1 * (CT(2) * u - CT(1)) + k2) * CT(0.5);
-    p = (k0 * (u * u + u) + k1 * (CT(2) * u + CT(1)) + k2) * CT(0.5);
+    // z = k0 (1-u^2) - 2u k1 - k2, m = (k0 (u^2-u) + k1 (2u-1) + k2)/2,
+    // p = (k0 (u^2+u) + k1 (2u+1) + k2)/2
+    const CT uu = u * u, tu = CT(2) * u;
+    z = mad(-tu, k1, k0 * (CT(1) - uu)) - k2;
+    m = (mad(k1, tu - CT(1), k0 * (uu - u)) + k2) * CT(0.5);
+    p = (mad(k1, tu + CT(1), k0 * (uu + u)) + k2) * CT(0.5);
 }
 
 template <class CT>
@@ -159,8 +192,8 @@ __device__ __forceinline__ CT cy_nu_from_central(CT Cxx, CT Cyy, CT Czz, CT Cxy,
 // `cy` non-null: the shear viscosity comes from the Carreau-Yasuda law evaluated on this
 // cell's own central second moments (k_200 ... k_011 of the forward transform); S receives
 // the strain rate
-template <class CT>
-__device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu, const CYParams<CT>* cy = nullptr,
+template <class CT, class PT = CT>
+__device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu, const CYParams<PT>* cy = nullptr,
                                             CT* S = nullptr)
 {
     // forward: z pass over the 9 (x,y) columns
@@ -186,7 +219,7 @@ __device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, 
             if (ky + kz <= 2) fwd3<CT>(b[0][ky][kz], b[1][ky][kz], b[2][ky][kz], ux, k[0][ky][kz], k[1][ky][kz], k[2][ky][kz]);
 
     const CT ir = CT(1) / rho;
-    if (cy) nu = cy_nu_from_central<CT>(k[2][0][0], k[0][2][0], k[0][0][2], k[1][1][0], k[1][0][1], k[0][1][1], rho, *cy, S);
+    if (cy) nu = cy_nu_from_central(k[2][0][0], k[0][2][0], k[0][0][2], k[1][1][0], k[1][0][1], k[0][1][1], rho, *cy, S);
     const CT om = CT(1) / (CT(3) * nu + CT(0.5));
     const CT k000 = k[0][0][0];
     // relaxation (lbm_col_cum.h:205-235 with omega2 = 1 and no anti-aliasing terms)
@@ -480,6 +513,19 @@ __device__ __forceinline__ CT cy_nu_from_central(CT Cxx, CT Cyy, CT Czz, CT Cxy,
     const CT sc = CT(-3) / (CT(2) * rho * tau);
     S[0] = sc * Pxx; S[1] = sc * Cxy; S[2] = sc * Cxz; S[3] = sc * Pyy; S[4] = sc * Cyz; S[5] = sc * Pzz;
     return (tau - CT(0.5)) * CT(1.0 / 3.0);
+}
+
+// two cells at once: the Newton solve runs per half (its branches and transcendental
+// functions are scalar)
+__device__ __forceinline__ f2 cy_nu_from_central(f2 Cxx, f2 Cyy, f2 Czz, f2 Cxy, f2 Cxz, f2 Cyz, f2 rho,
+                                                 const CYParams<float>& p, f2* S)
+{
+    float Sa[6], Sb[6];
+    const float na = cy_nu_from_central<float>(Cxx.v.x, Cyy.v.x, Czz.v.x, Cxy.v.x, Cxz.v.x, Cyz.v.x, rho.v.x, p, Sa);
+    const float nb = cy_nu_from_central<float>(Cxx.v.y, Cyy.v.y, Czz.v.y, Cxy.v.y, Cxz.v.y, Cyz.v.y, rho.v.y, p, Sb);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) S[k] = f2(Sa[k], Sb[k]);
+    return f2(na, nb);
 }
 
 // the same from the populations: raw second moments by additions only (c in {-1,0,1}),
