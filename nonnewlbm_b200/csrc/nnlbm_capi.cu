@@ -284,6 +284,14 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
             ch.cflags = (int)j | (ch.cflags & ~CH_CASE_MASK);
             chunks.push_back(ch);
         }
+        // a paired step kernel takes chunks two by two: an odd count gets an empty chunk,
+        // so that no pair mixes two cases
+        if (pairs_chunks(g.dtype, g.collision) && (c.chunks.size() & 1) && j + 1 < g.cases.size()) {
+            Chunk none = chunks.back();
+            none.fluid = 0;
+            none.periodic = 0;
+            chunks.push_back(none);
+        }
         for (int32_t k : c.gather_self)
             gather.push_back(make_int4(c.self_cell[k], (int)j, (int)(self_off + k), (int)c.label[c.self_cell[k]]));
         for (int32_t cell : c.self_cell) nodes.push_back(make_int2(cell, (int)j));
@@ -315,7 +323,7 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     g.n_self = self_off;
     GroupArgs<CT>& ga = *(GroupArgs<CT>*)g.args.data();
     memset(&ga, 0, sizeof ga);
-    ga.c0 = ca[0];
+    for (size_t j = 0; j < ca.size() && j < (size_t)kParamCases; ++j) ga.cp[j] = ca[j];
     ga.n_cases = (int)ca.size();
     ga.cases = (const CaseArgs<CT>*)g.d_cases;
     ga.chunks = g.d_chunks;

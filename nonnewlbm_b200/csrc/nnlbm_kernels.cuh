@@ -120,10 +120,13 @@ struct alignas(16) Chunk {
 // colliding cell at x = 0 or nx-1)
 enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PLAIN = 1 << 18 };
 
-// a launch group: cases sharing storage type and collision
+// a launch group: cases sharing storage type and collision.  Up to kParamCases cases also
+// travel in the kernel parameters (read through the constant cache, indexed by the
+// chunk's case); larger groups read them from the device array.
+constexpr int kParamCases = 32;
 template <class CT>
 struct GroupArgs {
-    CaseArgs<CT> c0;           // copy of case 0 in parameter space (single-case groups)
+    CaseArgs<CT> cp[kParamCases];  // copies of the first kParamCases cases in parameter space
     int n_cases, pad2;
     const CaseArgs<CT>* cases;
     const Chunk* chunks;
@@ -443,7 +446,10 @@ __device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseA
 }
 
 // the step kernel of a (storage, collision) pairs its plain chunks (fluid_pair) when the
-// arithmetic is single precision and the collision is the cumulant
+// arithmetic is single precision and the collision is the cumulant.  The host pads each
+// case's chunk list to an even length (but the last), so a pair never mixes two cases:
+// a chunk meets the same partner, and the same arithmetic, whether its case runs alone
+// or batched with others.
 __host__ __device__ constexpr bool pairs_chunks(int dt, int col) { return dt != 0 && col == COL_CUM; }
 
 // 32 boundary nodes (open-plane nodes and GEO_INFLOW nodes, one per lane): each writes
@@ -481,7 +487,7 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
 
 // the step kernel: one warp per chunk of the work list, then one warp per 32 boundary
 // nodes.  Both write only the slots their own cells read, so they run side by side.
-template <int DT, int COL, bool ODD, bool SINGLE>
+template <int DT, int COL, bool ODD, bool PARAM>
 __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
     k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
@@ -491,7 +497,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
     const int step = g.cursor[ODD ? 1 : 0];
     if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
     // the step's flags are the same for every case of the group
-    const int flags = (SINGLE ? g.c0.ctl : g.cases[0].ctl)[step].flags;
+    const int flags = (PARAM ? g.cp[0].ctl : g.cases[0].ctl)[step].flags;
     if constexpr (pairs_chunks(DT, COL)) {
         // warp w takes chunks 2w and 2w + 1; a pair that is not two plain chunks of one case
         // (without the finite-difference force) is stepped chunk by chunk
@@ -502,14 +508,14 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
             if (2 * w + 1 < g.n_chunks) cb = g.chunks[2 * w + 1];
             else cb.cflags = ca.cflags; // empty partner: no colliding lane
             const int ci = ca.cflags & CH_CASE_MASK;
-            const CaseArgs<CT>& a = SINGLE ? g.c0 : g.cases[ci];
+            const CaseArgs<CT>& a = PARAM ? g.cp[ci] : g.cases[ci];
             if (((ca.cflags & cb.cflags) & CH_PLAIN) && ci == (cb.cflags & CH_CASE_MASK) && a.cy_mode != CY_REF_FD) {
                 fluid_pair<DT, ODD>(a, g.cases + ci, ca, cb, step, flags, lane);
             } else {
                 fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, step, flags, lane);
                 if (cb.fluid) {
                     const int cj = cb.cflags & CH_CASE_MASK;
-                    fluid_chunk<DT, COL, ODD>(SINGLE ? g.c0 : g.cases[cj], g.cases + cj, cb, step, flags, lane);
+                    fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[cj] : g.cases[cj], g.cases + cj, cb, step, flags, lane);
                 }
             }
         } else {
@@ -519,7 +525,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
         if (w < g.n_chunks) {
             const Chunk ch = g.chunks[w];
             const int ci = ch.cflags & CH_CASE_MASK;
-            fluid_chunk<DT, COL, ODD>(SINGLE ? g.c0 : g.cases[ci], g.cases + ci, ch, step, flags, lane);
+            fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[ci] : g.cases[ci], g.cases + ci, ch, step, flags, lane);
         } else {
             node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
         }
@@ -673,10 +679,10 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
 using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 
 // launch of one step-kernel variant: one warp per chunk
-template <int DT, int COL, bool ODD, bool SINGLE>
+template <int DT, int COL, bool ODD, bool PARAM>
 void launch_step_variant(dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
-    k_step<DT, COL, ODD, SINGLE><<<grid, block, 0, s>>>(g);
+    k_step<DT, COL, ODD, PARAM><<<grid, block, 0, s>>>(g);
 }
 
 template <int DT, int COL>
@@ -684,7 +690,8 @@ void launch_step(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* ar
 {
     using CT = typename Storage<DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
-    if (g.n_cases == 1) {
+    // PARAM: the cases' arguments are in parameter space (g.cp)
+    if (g.n_cases <= kParamCases) {
         if (odd) launch_step_variant<DT, COL, true, true>(grid, block, s, g);
         else launch_step_variant<DT, COL, false, true>(grid, block, s, g);
     } else {
