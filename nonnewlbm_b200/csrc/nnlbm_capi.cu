@@ -186,6 +186,16 @@ void fill_case_args(const Case& c, CaseArgs<CT>& a)
     a.ctl = (const StepCtl<CT>*)c.d_ctl;
     a.red = c.d_red;
     a.err = c.d_err;
+    // slot bases (integer arithmetic: a shifted base may point before the array; the cell
+    // index of every plain access brings it back inside)
+    const uintptr_t base = (uintptr_t)c.df;
+    const int64_t S = kStorageBytes[c.d.dtype], qs = (int64_t)c.q_stride, sy = c.d.nx, sz = (int64_t)c.d.nx * c.d.ny;
+    for (int q = 0; q < 27; ++q) {
+        const int64_t sh = cxq(q) + cyq(q) * sy + czq(q) * sz;
+        a.slot_even[q] = (const void*)(base + (uintptr_t)(q * qs * S));
+        a.slot_odd_ld[q] = (const void*)(base + (uintptr_t)((oppq(q) * qs - sh) * S));
+        a.slot_odd_st[q] = (const void*)(base + (uintptr_t)((q * qs + sh) * S));
+    }
 }
 
 void rebuild_case_args(nnlbm_ctx* ctx, Case& c)

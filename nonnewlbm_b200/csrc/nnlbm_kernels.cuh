@@ -107,6 +107,14 @@ struct CaseArgs {
     const StepCtl<CT>* ctl;
     double* red;               // [5] mass, Q_ivc, Q_svc, Q_out5, Q_out6
     int* err;                  // watchdog flag
+    // per-slot base addresses of a plain chunk's accesses, each the population array of one
+    // slot already offset by the cell shift of the access, so that an address is one
+    // shift-and-add of the cell index: slot q (even step, loads of slot q and stores of
+    // slot opp(q)); slot opp(q) at -c_q (odd-step loads of direction q); slot q at +c_q
+    // (odd-step stores of direction q)
+    const void* slot_even[27];
+    const void* slot_odd_ld[27];
+    const void* slot_odd_st[27];
 };
 
 // one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
@@ -123,7 +131,7 @@ enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PL
 // a launch group: cases sharing storage type and collision.  Up to kParamCases cases also
 // travel in the kernel parameters (read through the constant cache, indexed by the
 // chunk's case); larger groups read them from the device array.
-constexpr int kParamCases = 32;
+constexpr int kParamCases = 16;
 template <class CT>
 struct GroupArgs {
     CaseArgs<CT> cp[kParamCases];  // copies of the first kParamCases cases in parameter space
@@ -314,12 +322,11 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         if (!ODD) {
             // slot q at c
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = S::from(pc[q * qs], q, a.inv_scale);
+            for (int q = 0; q < 27; ++q) f[q] = S::from(((const T*)a.slot_even[q])[c], q, a.inv_scale);
         } else if (plain) {
             // slot opp(q) at c - c_q
 #pragma unroll
-            for (int q = 0; q < 27; ++q)
-                f[q] = S::from(pc[oppq(q) * qs - (cxq(q) + cyq(q) * sy + czq(q) * sz)], q, a.inv_scale);
+            for (int q = 0; q < 27; ++q) f[q] = S::from(((const T*)a.slot_odd_ld[q])[c], q, a.inv_scale);
         } else {
 #pragma unroll
             for (int q = 0; q < 27; ++q) f[q] = S::from(pc[oppq(q) * qs + nbr(q, -1)], q, a.inv_scale);
@@ -341,11 +348,11 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         if (!ODD) {
             // slot opp(q) at c
 #pragma unroll
-            for (int q = 0; q < 27; ++q) S::store(ps, oppq(q) * qs, q, f[q], a.scale);
+            for (int q = 0; q < 27; ++q) S::store((T*)a.slot_even[oppq(q)], c, q, f[q], a.scale);
         } else if (plain) {
             // slot q at c + c_q
 #pragma unroll
-            for (int q = 0; q < 27; ++q) S::store(ps, q * qs + (cxq(q) + cyq(q) * sy + czq(q) * sz), q, f[q], a.scale);
+            for (int q = 0; q < 27; ++q) S::store((T*)a.slot_odd_st[q], c, q, f[q], a.scale);
         } else {
 #pragma unroll
             for (int q = 0; q < 27; ++q) S::store(ps, q * qs + nbr(q, 1), q, f[q], a.scale);
@@ -394,14 +401,12 @@ __device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseA
     if (fa || fb) {
         const int cA = ca.c0 + lane, cB = cb.c0 + lane;
         const int64_t qs = a.qstride, sy = a.nx, sz = (int64_t)a.nx * a.ny;
-        const T* pa = (const T*)a.df + cA;
-        const T* pb = (const T*)a.df + cB;
         const f2 isc(a.inv_scale);
         f2 f[27];
 #pragma unroll
         for (int q = 0; q < 27; ++q) {
-            const int64_t o = ODD ? oppq(q) * qs - (cxq(q) + cyq(q) * sy + czq(q) * sz) : q * qs;
-            const f2 raw(fa ? Raw<DT>::get(pa[o]) : 0.f, fb ? Raw<DT>::get(pb[o]) : 0.f);
+            const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
+            const f2 raw(fa ? Raw<DT>::get(p[cA]) : 0.f, fb ? Raw<DT>::get(p[cB]) : 0.f);
             const f2 w(weight<float>(q));
             f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
         }
@@ -410,16 +415,14 @@ __device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseA
         f2 Sl[6];
         const CYParams<float> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
         collide_cum<f2, float>(f, rho, ux, uy, uz, f2(a.nu), a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
-        T* qa = (T*)a.df + cA;
-        T* qb = (T*)a.df + cB;
         const f2 sc(a.scale);
 #pragma unroll
         for (int q = 0; q < 27; ++q) {
-            const int64_t o = ODD ? q * qs + (cxq(q) + cyq(q) * sy + czq(q) * sz) : oppq(q) * qs;
+            T* p = (T*)(ODD ? a.slot_odd_st[q] : a.slot_even[oppq(q)]);
             const f2 w(weight<float>(q));
             const f2 v = DT == 1 ? f[q] - w : (f[q] - w) * sc;
-            if (fa) qa[o] = Cook<DT>::put(v.v.x);
-            if (fb) qb[o] = Cook<DT>::put(v.v.y);
+            if (fa) p[cA] = Cook<DT>::put(v.v.x);
+            if (fb) p[cB] = Cook<DT>::put(v.v.y);
         }
         const float r[2] = {rho.v.x, rho.v.y}, u0[2] = {ux.v.x, ux.v.y}, u1[2] = {uy.v.x, uy.v.y}, u2[2] = {uz.v.x, uz.v.y};
         const bool on[2] = {fa, fb};
