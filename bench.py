@@ -66,15 +66,20 @@ class Dist:
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
 
-    def init(self):
+    def init(self, backend: str = "nccl"):
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", self.local))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
+            self.backend = backend
             self.pg = dist
 
     def barrier(self):
@@ -86,7 +91,8 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if getattr(self, "backend", "nccl") == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 

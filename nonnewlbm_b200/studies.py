@@ -132,6 +132,19 @@ def run_batch(cases: list[StudyCase], steps: int = 200, warmup: int = 20, device
             "scales": [round(c.scale, 4) for c in cases]}
 
 
+def shard_cases(cases: list, rank: int, world: int, size=lambda c: int(c.wall.size)) -> list:
+    """This rank's share of a batch split over `world` GPUs (one process each): the cases
+    are independent, so they are dealt out whole, largest first, each to the rank with the
+    least work so far; every rank computes the same split and no data crosses GPUs."""
+    load = [0] * world
+    owner = {}
+    for i in sorted(range(len(cases)), key=lambda i: (-size(cases[i]), i)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        owner[i] = r
+        load[r] += size(cases[i])
+    return [cases[i] for i in range(len(cases)) if owner[i] == rank]
+
+
 def _near_wall(wall_flags: np.ndarray) -> np.ndarray:
     wf = wall_flags
     near = np.zeros(wf.shape, dtype=bool)
