@@ -18,7 +18,7 @@
 #include "nnlbm_kernels.cuh"
 
 namespace nnlbm {
-#define NNLBM_DECL_STEP(DT, COL) void launch_step_##DT##_##COL(bool, dim3, dim3, cudaStream_t, const void*);
+#define NNLBM_DECL_STEP(DT, COL) void launch_step_##DT##_##COL(bool, bool, dim3, dim3, cudaStream_t, const void*);
 #define NNLBM_DECL_STEP_DT(DT)                                                                                        \
     NNLBM_DECL_STEP(DT, 0) NNLBM_DECL_STEP(DT, 1) NNLBM_DECL_STEP(DT, 2) NNLBM_DECL_STEP(DT, 3) NNLBM_DECL_STEP(DT, 4) \
     NNLBM_DECL_STEP(DT, 5) NNLBM_DECL_STEP(DT, 6) NNLBM_DECL_STEP(DT, 7) NNLBM_DECL_STEP(DT, 8) NNLBM_DECL_STEP(DT, 9) \
@@ -32,13 +32,13 @@ NNLBM_DECL_STEP_DT(0) NNLBM_DECL_STEP_DT(1) NNLBM_DECL_STEP_DT(2) NNLBM_DECL_STE
     void launch_init_macro_##DT(const void*, double, double, double, double, cudaStream_t);
 NNLBM_DECL_AUX(0) NNLBM_DECL_AUX(1) NNLBM_DECL_AUX(2) NNLBM_DECL_AUX(3)
 
-GroupLauncher step_launcher(int dt, int col)
+StepLauncher step_launcher(int dt, int col)
 {
 #define NNLBM_ROW(DT)                                                                                     \
     {launch_step_##DT##_0, launch_step_##DT##_1, launch_step_##DT##_2, launch_step_##DT##_3,             \
      launch_step_##DT##_4, launch_step_##DT##_5, launch_step_##DT##_6, launch_step_##DT##_7,             \
      launch_step_##DT##_8, launch_step_##DT##_9, launch_step_##DT##_10}
-    static const GroupLauncher table[4][11] = {NNLBM_ROW(0), NNLBM_ROW(1), NNLBM_ROW(2), NNLBM_ROW(3)};
+    static const StepLauncher table[4][11] = {NNLBM_ROW(0), NNLBM_ROW(1), NNLBM_ROW(2), NNLBM_ROW(3)};
     return table[dt][col];
 }
 
@@ -376,7 +376,7 @@ int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
         A.refd_stress(odd, rgrid, cblk, ctx->stream, g.args.data());
     }
     if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
-    step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, g.args.data());
+    step_launcher(g.dtype, g.collision)(odd, g.n_gather > 0, cgrid, cblk, ctx->stream, g.args.data());
     CK(cudaGetLastError());
     return NNLBM_OK;
 }
@@ -1149,7 +1149,7 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
             A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
             mark(0);
         }
-        step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, g.args.data());
+        step_launcher(g.dtype, g.collision)(odd, false, cgrid, cblk, ctx->stream, g.args.data());
         mark(1);
         CK(cudaGetLastError());
     }
@@ -1236,7 +1236,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
                 A.refd_stress(odd, rgrid, cblk, ctx->stream, args);
             }
             if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, args);
-            step_launcher(g.dtype, g.collision)(odd, cgrid, cblk, ctx->stream, args);
+            step_launcher(g.dtype, g.collision)(odd, false, cgrid, cblk, ctx->stream, args);
         }
         CK(cudaGetLastError());
         // pageable destination: the copy returns once the cursor is on the host; the last

@@ -150,6 +150,13 @@ struct GroupArgs {
     int* cursor;
 };
 
+// programmatic dependent launch (sm_90+): the open-plane gather lets the step kernel of the
+// same step start at once; the step kernel waits for the gather's completion (and its
+// memory) only before its first population store and before reading the gathered values.
+// Without the launch attribute the wait returns at once.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <int DT>
 __device__ __forceinline__ typename Storage<DT>::T* qptr(const CaseArgs<typename Storage<DT>::CT>& a, int q)
 {
@@ -344,6 +351,8 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         CT Sl[6];
         const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
         collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
+        // the gather of this step reads the slots written below
+        pdl_wait();
         T* ps = (T*)a.df + c;
         if (!ODD) {
             // slot opp(q) at c
@@ -415,6 +424,8 @@ __device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseA
         f2 Sl[6];
         const CYParams<float> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
         collide_cum<f2, float>(f, rho, ux, uy, uz, f2(a.nu), a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
+        // the gather of this step reads the slots written below
+        pdl_wait();
         const f2 sc(a.scale);
 #pragma unroll
         for (int q = 0; q < 27; ++q) {
@@ -464,6 +475,7 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
                                         int step, int flags)
 {
     using CT = typename Storage<DT>::CT;
+    pdl_wait(); // the gathered values
     if (k >= n_nodes) return;
     const int2 nd = nodes[k];
     const CaseArgs<CT>& a = cases[nd.y];
@@ -566,6 +578,7 @@ template <int DT, bool ODD>
 __global__ void __launch_bounds__(64) k_bc_gather(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
+    pdl_launch_dependents();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.n_gather) return;
     // {cell, case, node index, label}: the stencil loads depend on nothing but this record
@@ -680,29 +693,46 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
 // translation unit
 // ---------------------------------------------------------------------------------------
 using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
+// the step kernel's launcher: `after_gather` launches it as a programmatic dependent of the
+// gather kernel just enqueued on the stream
+using StepLauncher = void (*)(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 
 // launch of one step-kernel variant: one warp per chunk
 template <int DT, int COL, bool ODD, bool PARAM>
-void launch_step_variant(dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
+void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
-    k_step<DT, COL, ODD, PARAM><<<grid, block, 0, s>>>(g);
+    if (!after_gather) {
+        k_step<DT, COL, ODD, PARAM><<<grid, block, 0, s>>>(g);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_step<DT, COL, ODD, PARAM>, g);
 }
 
 template <int DT, int COL>
-void launch_step(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args)
+void launch_step(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
     // PARAM: the cases' arguments are in parameter space (g.cp)
     if (g.n_cases <= kParamCases) {
-        if (odd) launch_step_variant<DT, COL, true, true>(grid, block, s, g);
-        else launch_step_variant<DT, COL, false, true>(grid, block, s, g);
+        if (odd) launch_step_variant<DT, COL, true, true>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, true>(after_gather, grid, block, s, g);
     } else {
-        if (odd) launch_step_variant<DT, COL, true, false>(grid, block, s, g);
-        else launch_step_variant<DT, COL, false, false>(grid, block, s, g);
+        if (odd) launch_step_variant<DT, COL, true, false>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, false>(after_gather, grid, block, s, g);
     }
 }
 
-GroupLauncher step_launcher(int dtype, int collision);
+StepLauncher step_launcher(int dtype, int collision);
 
 } // namespace nnlbm
