@@ -54,8 +54,13 @@ void NNLBM_CAT(launch_bc_gather_, NNLBM_DT)(bool odd, dim3 grid, dim3 block, cud
 {
     using CT = typename Storage<NNLBM_DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
-    if (odd) k_bc_gather<NNLBM_DT, true><<<grid, block, 0, s>>>(g);
-    else k_bc_gather<NNLBM_DT, false><<<grid, block, 0, s>>>(g);
+    if (g.n_cases <= kParamCases) {
+        if (odd) k_bc_gather<NNLBM_DT, true, true><<<grid, block, 0, s>>>(g);
+        else k_bc_gather<NNLBM_DT, false, true><<<grid, block, 0, s>>>(g);
+    } else {
+        if (odd) k_bc_gather<NNLBM_DT, true, false><<<grid, block, 0, s>>>(g);
+        else k_bc_gather<NNLBM_DT, false, false><<<grid, block, 0, s>>>(g);
+    }
 }
 
 void NNLBM_CAT(launch_refd_velocity_, NNLBM_DT)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* args)

@@ -15,7 +15,7 @@
 // value f*_q = incoming f_opp(q) already sits in the slot the neighbour reads next.
 //
 // Work decomposition: a packed list of 32-cell row chunks of colliding cells (one warp
-// each, or one warp per two chunks for the single-precision cumulant), over all cases of
+// each, or one warp per two chunks in single-precision arithmetic), over all cases of
 // a launch group (same storage type and collision), followed by warps of 32 boundary
 // nodes.  Per-case parameters live in a device array indexed by the chunk's case (and in
 // parameter space for a single-case group).
@@ -285,15 +285,25 @@ __device__ __noinline__ void refd_force(const CaseArgs<CT>* ap, int c, int sy, i
     F[2] += CT(2) * (nuc - a.nu) * F3;
 }
 
+// the step kernel of a (storage, collision) pairs its plain chunks when the arithmetic is
+// single precision and the collision is the cumulant, BGK or MRT (KBC's moment sets need
+// too many registers for two cells a thread).  The host pads each case's chunk list to
+// an even length, so a pair never mixes two cases: a chunk meets the same partner, and
+// the same arithmetic, whether its case runs alone or batched with others.
+__host__ __device__ constexpr bool pairs_chunks(int dt, int col)
+{
+    return dt != 0 && (col == COL_CUM || col == COL_BGK || col == COL_MRT);
+}
+
 // register budget per thread of each step-kernel variant: FP64 arithmetic may use all
-// 255; the paired cumulant (two cells per thread) gets NNLBM_PAIR_REGS; everything else
+// 255; the paired variants (two cells per thread) get NNLBM_PAIR_REGS; everything else
 // 128, two 256-thread blocks per SM
 #ifndef NNLBM_PAIR_REGS
 #define NNLBM_PAIR_REGS 128
 #endif
 template <int DT, int COL>
 struct StepRegs {
-    static constexpr int value = DT == 0 ? 255 : COL == COL_CUM ? NNLBM_PAIR_REGS : 128;
+    static constexpr int value = DT == 0 ? 255 : pairs_chunks(DT, COL) ? NNLBM_PAIR_REGS : 128;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -384,24 +394,22 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
 }
 
 // ---------------------------------------------------------------------------------------
-// two plain chunks of one case in one warp, one cell of each per lane, for the cumulant
-// in single-precision arithmetic: the two cells' arithmetic runs as f2 on the packed
+// two plain chunks of one case in one warp, one cell of each per lane, for the cumulant,
+// BGK and MRT in single-precision arithmetic: the two cells' arithmetic runs as f2 on the packed
 // FP32 pipe, so the pair issues about the FP32 instructions of one cell; loads, stores
 // and the per-cell outputs stay per cell.  A lane whose cell in one chunk does not
 // collide computes that half from the rest state and stores nothing for it.
 // ---------------------------------------------------------------------------------------
-template <int DT> struct Raw;
-template <> struct Raw<1> { __device__ static __forceinline__ float get(float v) { return v; } };
-template <> struct Raw<2> { __device__ static __forceinline__ float get(__half v) { return __half2float(v); } };
-template <> struct Raw<3> { __device__ static __forceinline__ float get(__nv_bfloat16 v) { return __bfloat162float(v); } };
 template <int DT> struct Cook;
 template <> struct Cook<1> { __device__ static __forceinline__ float put(float v) { return v; } };
 template <> struct Cook<2> { __device__ static __forceinline__ __half put(float v) { return __float2half_rn(v); } };
 template <> struct Cook<3> { __device__ static __forceinline__ __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); } };
 
-template <int DT, bool ODD>
-__device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseArgs<float>* ap, const Chunk& ca, const Chunk& cb,
-                                           int step, int flags, int lane)
+// the rest of a pair once its populations f (raw stored value + weight, or the rest state
+// where the cell does not collide) are in registers: collision, stores, per-cell outputs
+template <int DT, int COL, bool ODD>
+__device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, f2* f, int step,
+                                            int flags, int lane)
 {
     using T = typename Storage<DT>::T;
     const unsigned bit = 1u << lane;
@@ -409,21 +417,12 @@ __device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseA
     double mass = 0.0;
     if (fa || fb) {
         const int cA = ca.c0 + lane, cB = cb.c0 + lane;
-        const int64_t qs = a.qstride, sy = a.nx, sz = (int64_t)a.nx * a.ny;
-        const f2 isc(a.inv_scale);
-        f2 f[27];
-#pragma unroll
-        for (int q = 0; q < 27; ++q) {
-            const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
-            const f2 raw(fa ? Raw<DT>::get(p[cA]) : 0.f, fb ? Raw<DT>::get(p[cB]) : 0.f);
-            const f2 w(weight<float>(q));
-            f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
-        }
+        const f2 fx(a.fx), fy(a.fy), fz(a.fz);
         f2 rho, ux, uy, uz;
-        density_velocity<f2>(f, f2(a.fx), f2(a.fy), f2(a.fz), rho, ux, uy, uz);
+        density_velocity<f2>(f, fx, fy, fz, rho, ux, uy, uz);
         f2 Sl[6];
         const CYParams<float> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
-        collide_cum<f2, float>(f, rho, ux, uy, uz, f2(a.nu), a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
+        collide<f2, COL, float>(f, rho, ux, uy, uz, fx, fy, fz, f2(a.nu), a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
         // the gather of this step reads the slots written below
         pdl_wait();
         const f2 sc(a.scale);
@@ -459,12 +458,91 @@ __device__ __forceinline__ void fluid_pair(const CaseArgs<float>& a, const CaseA
     }
 }
 
-// the step kernel of a (storage, collision) pairs its plain chunks (fluid_pair) when the
-// arithmetic is single precision and the collision is the cumulant.  The host pads each
-// case's chunk list to an even length (but the last), so a pair never mixes two cases:
-// a chunk meets the same partner, and the same arithmetic, whether its case runs alone
-// or batched with others.
-__host__ __device__ constexpr bool pairs_chunks(int dt, int col) { return dt != 0 && col == COL_CUM; }
+// ---------------------------------------------------------------------------------------
+// the paired step as a software pipeline: while a warp collides one pair, the next pair's
+// populations travel into the warp's staging buffer in shared memory (cp.async, one
+// 32-bit word per value and lane: word [q][h][lane] holds the raw stored value of cell h,
+// zero where that cell does not collide; 16-bit storage copies the aligned word around
+// the value), and the chunk records of the pair after that come in behind them.
+// ---------------------------------------------------------------------------------------
+struct alignas(16) PairStage {
+    uint32_t pop[27 * 64];
+    Chunk rec[3][2]; // a ring of three record pairs
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+// 4 bytes from src, or zeros (nothing read) when !on
+__device__ __forceinline__ void cp_async4(uint32_t* dst, const void* src, bool on)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(on ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// the 32-bit word holding element p (16-bit storage: the aligned pair around it)
+template <class T>
+__device__ __forceinline__ const void* word_of(const T* p)
+{
+    return sizeof(T) == 4 ? (const void*)p : (const void*)((uintptr_t)p & ~(uintptr_t)3);
+}
+// the value of element p out of its staged word
+template <int DT>
+__device__ __forceinline__ float raw_of(uint32_t wd, const typename Storage<DT>::T* p)
+{
+    if constexpr (DT == 1) {
+        return __uint_as_float(wd);
+    } else {
+        const unsigned short h = (unsigned short)(((uintptr_t)p & 2) ? (wd >> 16) : (wd & 0xffffu));
+        if constexpr (DT == 2) return __half2float(__ushort_as_half(h));
+        else return __bfloat162float(__ushort_as_bfloat16(h));
+    }
+}
+
+template <int DT, bool ODD>
+__device__ __forceinline__ void stage_pair(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, uint32_t* pop, int lane)
+{
+    using T = typename Storage<DT>::T;
+    const unsigned bit = 1u << lane;
+    const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
+    const int cA = ca.c0 + lane, cB = cb.c0 + lane;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
+        // a cell that does not collide reads nothing (its address may leave the box)
+        cp_async4(pop + q * 64 + lane, fa ? word_of(p + cA) : a.df, fa);
+        cp_async4(pop + q * 64 + 32 + lane, fb ? word_of(p + cB) : a.df, fb);
+    }
+}
+
+template <int DT, bool ODD>
+__device__ __forceinline__ void unstage_pair(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, const uint32_t* pop,
+                                             int lane, f2* f)
+{
+    using T = typename Storage<DT>::T;
+    const int cA = ca.c0 + lane, cB = cb.c0 + lane;
+    const f2 isc(a.inv_scale);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
+        const f2 raw(raw_of<DT>(pop[q * 64 + lane], p + cA), raw_of<DT>(pop[q * 64 + 32 + lane], p + cB));
+        const f2 w(weight<float>(q));
+        f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
+    }
+}
+
+// two plain chunks of one case (no finite-difference force) collide as a pair
+template <bool PARAM>
+__device__ __forceinline__ bool pairable(const GroupArgs<float>& g, const Chunk& ca, const Chunk& cb)
+{
+    const int ci = ca.cflags & CH_CASE_MASK;
+    return ((ca.cflags & cb.cflags) & CH_PLAIN) && ci == (cb.cflags & CH_CASE_MASK) &&
+           (PARAM ? g.cp[ci] : g.cases[ci]).cy_mode != CY_REF_FD;
+}
 
 // 32 boundary nodes (open-plane nodes and GEO_INFLOW nodes, one per lane): each writes
 // the equilibrium of its gathered (rho, u) (or of its prescribed inflow) into its own
@@ -500,42 +578,87 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
     }
 }
 
+// a pair that is not pairable, chunk by chunk from direct loads (kept out of line: the
+// pipelined loop's own registers stay free of its needs)
+template <int DT, int COL, bool ODD, bool PARAM>
+__device__ __noinline__ void chunk_by_chunk(const GroupArgs<typename Storage<DT>::CT>& g, const Chunk ca, const Chunk cb,
+                                            int step, int flags, int lane)
+{
+    const int ci = ca.cflags & CH_CASE_MASK, cj = cb.cflags & CH_CASE_MASK;
+    fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[ci] : g.cases[ci], g.cases + ci, ca, step, flags, lane);
+    if (cb.fluid) fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[cj] : g.cases[cj], g.cases + cj, cb, step, flags, lane);
+}
+
 // the step kernel: one warp per chunk of the work list, then one warp per 32 boundary
 // nodes.  Both write only the slots their own cells read, so they run side by side.
+//
+// Paired variants run as a grid-stride loop over pairs (the host launches at most the
+// resident grid) with one PairStage of dynamic shared memory per warp: pair j + W is
+// staged while pair j collides, so only a warp's first pair waits for HBM.  A pair that
+// is not pairable (a face chunk, two cases, the finite-difference force) is stepped
+// chunk by chunk from direct loads, and the warps past the pairs take the node batches.
 template <int DT, int COL, bool ODD, bool PARAM>
 __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
     k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
     const int lane = threadIdx.x & 31;
-    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int step = g.cursor[ODD ? 1 : 0];
     if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
     // the step's flags are the same for every case of the group
     const int flags = (PARAM ? g.cp[0].ctl : g.cases[0].ctl)[step].flags;
     if constexpr (pairs_chunks(DT, COL)) {
-        // warp w takes chunks 2w and 2w + 1; a pair that is not two plain chunks of one case
-        // (without the finite-difference force) is stepped chunk by chunk
-        const int np = (g.n_chunks + 1) >> 1;
+        extern __shared__ PairStage stage_mem[];
+        PairStage& st = stage_mem[threadIdx.x >> 5];
+        const int nw = (int)(gridDim.x * (blockDim.x >> 5));
+        const int np = g.n_chunks >> 1; // the host pads the list to an even length
+        const int nj = np + (g.n_nodes + 31) / 32;
+        // lanes 0-3 copy the 64-byte record pair of pair j into ring slot r
+        auto fetch_records = [&](int j, int r) {
+            if (j < np && lane < 4) cp_async16((char*)st.rec[r] + 16 * lane, (const char*)(g.chunks + 2 * j) + 16 * lane);
+        };
+        auto case_of = [&](const Chunk& c) -> const CaseArgs<CT>& {
+            return PARAM ? g.cp[c.cflags & CH_CASE_MASK] : g.cases[c.cflags & CH_CASE_MASK];
+        };
+        // prologue: the records of the warp's first two pairs, then the first pair's populations
+        fetch_records(w, 0);
+        fetch_records(w + nw, 1);
+        cp_async_wait_all();
+        __syncwarp();
         if (w < np) {
-            const Chunk ca = g.chunks[2 * w];
-            Chunk cb{};
-            if (2 * w + 1 < g.n_chunks) cb = g.chunks[2 * w + 1];
-            else cb.cflags = ca.cflags; // empty partner: no colliding lane
-            const int ci = ca.cflags & CH_CASE_MASK;
-            const CaseArgs<CT>& a = PARAM ? g.cp[ci] : g.cases[ci];
-            if (((ca.cflags & cb.cflags) & CH_PLAIN) && ci == (cb.cflags & CH_CASE_MASK) && a.cy_mode != CY_REF_FD) {
-                fluid_pair<DT, ODD>(a, g.cases + ci, ca, cb, step, flags, lane);
-            } else {
-                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, step, flags, lane);
-                if (cb.fluid) {
-                    const int cj = cb.cflags & CH_CASE_MASK;
-                    fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[cj] : g.cases[cj], g.cases + cj, cb, step, flags, lane);
-                }
-            }
-        } else {
-            node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - np) * 32 + lane, step, flags);
+            const Chunk ca = st.rec[0][0], cb = st.rec[0][1];
+            if (pairable<PARAM>(g, ca, cb)) stage_pair<DT, ODD>(case_of(ca), ca, cb, st.pop, lane);
         }
+        cp_async_commit();
+        // ring slots: r holds this pair's records, r + 1 the next pair's, r + 2 receives the
+        // records of the pair after that
+        int r = 0;
+        for (; w < np; w += nw) {
+            const int wn = w + nw;
+            const int r1 = r == 2 ? 0 : r + 1, r2 = r1 == 2 ? 0 : r1 + 1;
+            // this pair's populations and the next pair's records have landed
+            cp_async_wait_all();
+            __syncwarp();
+            const Chunk ca = st.rec[r][0], cb = st.rec[r][1];
+            const bool staged = pairable<PARAM>(g, ca, cb);
+            const CaseArgs<CT>& a = case_of(ca);
+            f2 f[27];
+            if (staged) unstage_pair<DT, ODD>(a, ca, cb, st.pop, lane, f);
+            __syncwarp(); // every lane holds its words: the population buffer is free
+            if (wn < np) {
+                const Chunk na = st.rec[r1][0], nb = st.rec[r1][1];
+                if (pairable<PARAM>(g, na, nb)) stage_pair<DT, ODD>(case_of(na), na, nb, st.pop, lane);
+            }
+            fetch_records(wn + nw, r2);
+            cp_async_commit();
+            if (staged) pair_finish<DT, COL, ODD>(a, ca, cb, f, step, flags, lane);
+            else chunk_by_chunk<DT, COL, ODD, PARAM>(g, ca, cb, step, flags, lane);
+            r = r1;
+        }
+        // the node batches follow the pairs
+        for (; w < nj; w += nw)
+            node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - np) * 32 + lane, step, flags);
     } else {
         if (w < g.n_chunks) {
             const Chunk ch = g.chunks[w];
@@ -574,7 +697,7 @@ __device__ __forceinline__ void pull_triples(const CaseArgs<typename Storage<DT>
     for (int q = 0; q < 27; ++q) f[q] = canon<DT, ODD>(a, xs[1 - cxq(q)], ys[1 - cyq(q)], zs[1 - czq(q)], q);
 }
 
-template <int DT, bool ODD>
+template <int DT, bool ODD, bool PARAM>
 __global__ void __launch_bounds__(64) k_bc_gather(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
@@ -582,8 +705,9 @@ __global__ void __launch_bounds__(64) k_bc_gather(const __grid_constant__ GroupA
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.n_gather) return;
     // {cell, case, node index, label}: the stencil loads depend on nothing but this record
+    // (and the case's arguments, from the parameters where the group is small)
     const int4 e = g.gather[t];
-    const CaseArgs<CT>& a = g.cases[e.y];
+    const CaseArgs<CT>& a = PARAM ? g.cp[e.y] : g.cases[e.y];
     const StepCtl<CT>& ctl = a.ctl[g.cursor[ODD ? 1 : 0]];
     const int c = e.x, k = e.z;
     const int lab = e.w;
@@ -697,18 +821,27 @@ using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, 
 // gather kernel just enqueued on the stream
 using StepLauncher = void (*)(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 
-// launch of one step-kernel variant: one warp per chunk
+// dynamic shared memory of one step-kernel block: a PairStage per warp where the variant
+// pairs its chunks
+template <int DT, int COL>
+constexpr size_t step_smem(unsigned block)
+{
+    return pairs_chunks(DT, COL) ? (size_t)(block / 32) * sizeof(PairStage) : 0;
+}
+
+// launch of one step-kernel variant: one warp per chunk (per pair, grid-stride)
 template <int DT, int COL, bool ODD, bool PARAM>
 void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
+    const size_t smem = step_smem<DT, COL>(block.x);
     if (!after_gather) {
-        k_step<DT, COL, ODD, PARAM><<<grid, block, 0, s>>>(g);
+        k_step<DT, COL, ODD, PARAM><<<grid, block, smem, s>>>(g);
         return;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -733,6 +866,35 @@ void launch_step(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_
     }
 }
 
+// set-up of the four step-kernel variants of a (storage, collision) for blocks of `block`
+// threads, outside any stream capture: the dynamic shared memory limit of the paired
+// variants; returns how many such blocks one SM holds (0: none fits), or -1 for variants
+// that are not grid-stride (their grid is one warp per work item)
+template <int DT, int COL, bool ODD, bool PARAM>
+int prepare_step_variant(int block)
+{
+    const size_t smem = step_smem<DT, COL>((unsigned)block);
+    if (cudaFuncSetAttribute(k_step<DT, COL, ODD, PARAM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<DT, COL, ODD, PARAM>, block, smem) != cudaSuccess) return 0;
+    return n;
+}
+template <int DT, int COL>
+int prepare_step(int block)
+{
+    if constexpr (!pairs_chunks(DT, COL)) {
+        return -1;
+    } else {
+        const int n[4] = {prepare_step_variant<DT, COL, false, false>(block), prepare_step_variant<DT, COL, false, true>(block),
+                          prepare_step_variant<DT, COL, true, false>(block), prepare_step_variant<DT, COL, true, true>(block)};
+        return std::min(std::min(n[0], n[1]), std::min(n[2], n[3]));
+    }
+}
+using StepPrep = int (*)(int block);
+
 StepLauncher step_launcher(int dtype, int collision);
+StepPrep step_prep(int dtype, int collision);
 
 } // namespace nnlbm

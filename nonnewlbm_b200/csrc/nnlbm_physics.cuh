@@ -54,6 +54,7 @@ __device__ __forceinline__ f2 operator-(f2 a) { return __fmul2_rn(a.v, make_floa
 __device__ __forceinline__ f2 operator/(f2 a, f2 b) { return f2(a.v.x / b.v.x, a.v.y / b.v.y); }
 __device__ __forceinline__ f2& operator+=(f2& a, f2 b) { return a = a + b; }
 __device__ __forceinline__ f2& operator-=(f2& a, f2 b) { return a = a - b; }
+template <> __device__ __forceinline__ f2 dsqrt<f2>(f2 v) { return f2(sqrtf(v.v.x), sqrtf(v.v.y)); }
 
 // a b + c: one rounding for f2 (FFMA2); for float the compiler contracts it under
 // --use_fast_math; for double (built with -fmad=false) it is the product, then the sum,
@@ -317,7 +318,7 @@ __device__ __forceinline__ void collide_bgk(CT* f, CT rho, CT ux, CT uy, CT uz, 
 template <class CT>
 __device__ __forceinline__ void collide_mrt(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu)
 {
-    CT Pxx = 0, Pyy = 0, Pzz = 0, Pxy = 0, Pxz = 0, Pyz = 0;
+    CT Pxx = CT(0), Pyy = CT(0), Pzz = CT(0), Pxy = CT(0), Pxz = CT(0), Pyz = CT(0);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const int cx = cxq(q), cy = cyq(q), cz = czq(q);
@@ -364,7 +365,7 @@ template <class CT, bool USE_T, bool USE_Q>
 __device__ __forceinline__ CT kbc_shear(int q, const KbcMom<CT>& m)
 {
     const int cx = cxq(q), cy = cyq(q), cz = czq(q), nz0 = nnzq(q);
-    CT D = 0, T = 0, Qv = 0;
+    CT D = CT(0), T = CT(0), Qv = CT(0);
     if (nz0 == 1) {
         if (cx) D = (CT(2) * m.Nxz - m.Nyz) * CT(1.0 / 6.0);
         if (cy) D = (-m.Nxz + CT(2) * m.Nyz) * CT(1.0 / 6.0);
@@ -385,11 +386,24 @@ __device__ __forceinline__ CT kbc_shear(int q, const KbcMom<CT>& m)
     return D + (USE_T ? T : CT(0)) + (USE_Q ? Qv : CT(0));
 }
 
+// the entropic stabiliser gamma = 1/beta - (2 - 1/beta) num/den; the reference divides 0/0
+// when dh vanishes identically, where gamma*dh is zero for any finite gamma and the
+// regularised limit 1/beta is taken
+template <class CT>
+__device__ __forceinline__ CT kbc_gamma(CT num, CT den, CT beta)
+{
+    return den != CT(0) ? CT(1) / beta - (CT(2) - CT(1) / beta) * num / den : CT(1) / beta;
+}
+__device__ __forceinline__ f2 kbc_gamma(f2 num, f2 den, f2 beta)
+{
+    return f2(kbc_gamma<float>(num.v.x, den.v.x, beta.v.x), kbc_gamma<float>(num.v.y, den.v.y, beta.v.y));
+}
+
 template <class CT, bool CENTRAL, bool USE_T, bool USE_Q>
 __device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz, CT nu)
 {
-    CT M200 = 0, M020 = 0, M002 = 0, M110 = 0, M101 = 0, M011 = 0, M111 = 0;
-    CT M201 = 0, M102 = 0, M210 = 0, M120 = 0, M021 = 0, M012 = 0;
+    CT M200 = CT(0), M020 = CT(0), M002 = CT(0), M110 = CT(0), M101 = CT(0), M011 = CT(0), M111 = CT(0);
+    CT M201 = CT(0), M102 = CT(0), M210 = CT(0), M120 = CT(0), M021 = CT(0), M012 = CT(0);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const int cx = cxq(q), cy = cyq(q), cz = czq(q);
@@ -426,11 +440,12 @@ __device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, 
         m.Qxzz = M102 - CT(1.0 / 3.0) * (CT(6) * uz * cPxz + ux * (CT(3) * uz * uz - cNyz - cNxz + cT));
         m.Qyzz = M012 - CT(1.0 / 3.0) * (CT(6) * uz * cPyz + uy * (CT(3) * uz * uz - cNyz - cNxz + cT));
         m.Qxyz = M111 - ux * cPyz - uy * cPxz - uz * cPxy - ux * uy * uz;
-        e = {rho * CT(3) * cs2, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const CT z = CT(0);
+        e = {rho * CT(3) * cs2, z, z, z, z, z, z, z, z, z, z, z, z};
     }
     const FactEq<CT> E(ux, uy, uz);
     const CT beta = CT(1) / (CT(2) * nu / cs2 + CT(1));
-    CT num = 0, den = 0;
+    CT num = CT(0), den = CT(0);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const CT feq = E(q, rho);
@@ -440,9 +455,7 @@ __device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, 
         num += ds * dh * ifeq;
         den += dh * dh * ifeq;
     }
-    // the reference divides 0/0 when dh vanishes identically; gamma*dh is then zero for any
-    // finite gamma and the regularised limit 1/beta is taken
-    const CT gamma = den != CT(0) ? CT(1) / beta - (CT(2) - CT(1) / beta) * num / den : CT(1) / beta;
+    const CT gamma = kbc_gamma(num, den, beta);
     const CT ir = CT(1) / rho;
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
@@ -453,18 +466,19 @@ __device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, 
     }
 }
 
-template <class CT>
-__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, const CYParams<CT>& p, CT* S);
+template <class CT, class PT>
+__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, const CYParams<PT>& p, CT* S);
 
-// one collision; with `cy` the shear viscosity is the local Carreau-Yasuda one
-template <class CT, int COL>
+// one collision; with `cy` the shear viscosity is the local Carreau-Yasuda one.  CT is
+// the arithmetic type (f2: two cells at once), PT that of the viscosity-law parameters
+template <class CT, int COL, class PT = CT>
 __device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT fx, CT fy, CT fz, CT nu,
-                                        const CYParams<CT>* cy = nullptr, CT* S = nullptr)
+                                        const CYParams<PT>* cy = nullptr, CT* S = nullptr)
 {
     if constexpr (COL != COL_CUM) {
-        if (cy) nu = local_nu<CT>(f, rho, ux, uy, uz, *cy, S);
+        if (cy) nu = local_nu<CT, PT>(f, rho, ux, uy, uz, *cy, S);
     }
-    if constexpr (COL == COL_CUM) collide_cum<CT>(f, rho, ux, uy, uz, nu, cy, S);
+    if constexpr (COL == COL_CUM) collide_cum<CT, PT>(f, rho, ux, uy, uz, nu, cy, S);
     else if constexpr (COL == COL_MRT) collide_mrt<CT>(f, rho, ux, uy, uz, nu);
     else if constexpr (COL == COL_BGK) collide_bgk<CT>(f, rho, ux, uy, uz, fx, fy, fz, nu);
     else {
@@ -530,10 +544,10 @@ __device__ __forceinline__ f2 cy_nu_from_central(f2 Cxx, f2 Cyy, f2 Czz, f2 Cxy,
 
 // the same from the populations: raw second moments by additions only (c in {-1,0,1}),
 // shifted to central ones with the raw momentum j: C_ab = M_ab - u_a j_b - u_b j_a + rho u_a u_b
-template <class CT>
-__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, const CYParams<CT>& p, CT* S)
+template <class CT, class PT>
+__device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz, const CYParams<PT>& p, CT* S)
 {
-    CT Mxx = 0, Myy = 0, Mzz = 0, Mxy = 0, Mxz = 0, Myz = 0, jx = 0, jy = 0, jz = 0;
+    CT Mxx = CT(0), Myy = CT(0), Mzz = CT(0), Mxy = CT(0), Mxz = CT(0), Myz = CT(0), jx = CT(0), jy = CT(0), jz = CT(0);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const int cx = cxq(q), cy = cyq(q), cz = czq(q);
@@ -551,7 +565,7 @@ __device__ __forceinline__ CT local_nu(const CT* f, CT rho, CT ux, CT uy, CT uz,
     const CT Cxy = Mxy - ux * jy - uy * jx + rho * ux * uy;
     const CT Cxz = Mxz - ux * jz - uz * jx + rho * ux * uz;
     const CT Cyz = Myz - uy * jz - uz * jy + rho * uy * uz;
-    return cy_nu_from_central<CT>(Cxx, Cyy, Czz, Cxy, Cxz, Cyz, rho, p, S);
+    return cy_nu_from_central(Cxx, Cyy, Czz, Cxy, Cxz, Cyz, rho, p, S);
 }
 
 } // namespace nnlbm
