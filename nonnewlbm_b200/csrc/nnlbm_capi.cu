@@ -107,8 +107,8 @@ struct Case {
     void* d_stats = nullptr;
     void* d_ctl = nullptr;
     int64_t ctl_cap = 0;
-    double* d_red = nullptr;
-    int* d_err = nullptr;
+    double* d_red = nullptr;         // in the context's status block
+    int* d_err = nullptr;            // in the context's status block
     // host state
     std::vector<uint8_t> label;      // plain solver labels
     std::vector<uint8_t> dlabel;     // labels with the work flags of the device copy
@@ -141,7 +141,7 @@ struct Group {
     void* d_bc_prof = nullptr;
     void* d_bc_buf = nullptr;
     int64_t n_self = 0;
-    int* d_ints = nullptr;           // the two step cursors (one per A-A parity)
+    int* d_ints = nullptr;           // the two step cursors (one per A-A parity), in the status block
     bool any_refd = false;
     int block = 256;
     // the paired step kernel is grid-stride: at most max_blocks blocks of `block` threads
@@ -154,6 +154,15 @@ struct Group {
 
 } // namespace
 
+// every word the host reads back after a step, in one device block (and one pinned host
+// mirror) so that a synchronous step costs one small copy: per launch group 4 ints (the
+// two step cursors), per case 2 ints (the watchdog flag) and 8 doubles (the reductions)
+struct StatusLayout {
+    size_t cur, err, red, bytes;
+    explicit StatusLayout(size_t n_slots)
+        : cur(0), err(16 * n_slots), red(24 * n_slots), bytes(88 * n_slots) {}
+};
+
 struct nnlbm_ctx {
     int device = 0;
     int n_sm = 0;
@@ -161,6 +170,9 @@ struct nnlbm_ctx {
     std::vector<Case> cases;
     std::vector<Group> groups;
     std::string err;
+    char* d_status = nullptr;        // StatusLayout(cases.size()) on the device
+    char* h_status = nullptr;        // its pinned host mirror
+    bool status_fresh = false;       // the mirror holds the block as the last step left it
 };
 
 namespace {
@@ -447,6 +459,7 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags)
 {
     int rc;
     int64_t parity = -1;
+    ctx->status_fresh = false;
     for (int ic : g.cases) {
         Case& c = ctx->cases[ic];
         if (!c.has_map || !c.has_state) return set_err(ctx, NNLBM_ERR_ARG, "case %d has no map or initial state", ic);
@@ -499,23 +512,37 @@ int run_group_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool use_gra
     return NNLBM_OK;
 }
 
+// the status block into its host mirror: one copy, one wait
+int read_status(nnlbm_ctx* ctx)
+{
+    CK(cudaMemcpyAsync(ctx->h_status, ctx->d_status, StatusLayout(ctx->cases.size()).bytes, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->status_fresh = true;
+    return NNLBM_OK;
+}
+
+int check_watchdog(nnlbm_ctx* ctx)
+{
+    const StatusLayout sl(ctx->cases.size());
+    const int* err = (const int*)(ctx->h_status + sl.err);
+    for (size_t i = 0; i < ctx->cases.size(); ++i)
+        if (err[2 * i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
+    return NNLBM_OK;
+}
+
 int wait_and_check(nnlbm_ctx* ctx, int64_t n)
 {
-    std::vector<int> cur(ctx->groups.size() * 2), err(ctx->cases.size());
-    for (size_t i = 0; i < ctx->groups.size(); ++i)
-        CK(cudaMemcpyAsync(&cur[2 * i], ctx->groups[i].d_ints, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    for (size_t i = 0; i < ctx->cases.size(); ++i)
-        CK(cudaMemcpyAsync(&err[i], ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    int rc = read_status(ctx);
+    if (rc != NNLBM_OK) return rc;
+    const int* cur = (const int*)(ctx->h_status + StatusLayout(ctx->cases.size()).cur);
     for (size_t i = 0; i < ctx->groups.size(); ++i) {
         // the last step stored n into the cursor of the parity the group is at now
-        const int k = 2 * (int)i + (int)(ctx->cases[ctx->groups[i].cases[0]].parity & 1);
+        const int k = 4 * (int)i + (int)(ctx->cases[ctx->groups[i].cases[0]].parity & 1);
         if (cur[k] != n)
             return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", i, cur[k], (long long)n);
     }
-    for (size_t i = 0; i < ctx->cases.size(); ++i)
-        if (err[i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
-    return NNLBM_OK;
+    return check_watchdog(ctx);
 }
 
 bool is_pull_bc(int lab) { return lab == L_IN_L || lab == L_IN_R || lab == L_OUT_F || lab == L_OUT_B || lab == L_OUT_REQ; }
@@ -652,6 +679,13 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
         cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         return set_err(ctx, NNLBM_ERR_CUDA, "cannot initialise device %d", device);
     ctx->cases.resize(n_cases);
+    // a group per case at most
+    const StatusLayout sl((size_t)n_cases);
+    if (cudaMalloc(&ctx->d_status, sl.bytes) != cudaSuccess || cudaMallocHost(&ctx->h_status, sl.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, NNLBM_ERR_OOM, "allocation of the %zu-byte status block failed", sl.bytes);
+    }
+    cudaMemset(ctx->d_status, 0, sl.bytes);
     for (int i = 0; i < n_cases; ++i) {
         Case& c = ctx->cases[i];
         c.d = desc[i];
@@ -671,14 +705,13 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
         const size_t eb = kStorageBytes[d.dtype];
         c.q_stride = ((size_t)c.N + 127) / 128 * 128;
         if (cudaMalloc(&c.df_base, 27 * c.q_stride * eb + 2 * kDfPad) != cudaSuccess ||
-            cudaMalloc(&c.d_label, ((size_t)c.N + kLabelPad + 15) / 16 * 16) != cudaSuccess ||
-            cudaMalloc(&c.d_red, 8 * sizeof(double)) != cudaSuccess || cudaMalloc(&c.d_err, sizeof(int)) != cudaSuccess) {
+            cudaMalloc(&c.d_label, ((size_t)c.N + kLabelPad + 15) / 16 * 16) != cudaSuccess) {
             cudaGetLastError();
             return set_err(ctx, NNLBM_ERR_OOM, "case %d: device allocation of %.2f GB failed", i, 27.0 * c.q_stride * eb / 1e9);
         }
         c.df = (char*)c.df_base + kDfPad;
-        cudaMemset(c.d_red, 0, 8 * sizeof(double));
-        cudaMemset(c.d_err, 0, sizeof(int));
+        c.d_err = (int*)(ctx->d_status + sl.err) + 2 * i;
+        c.d_red = (double*)(ctx->d_status + sl.red) + 8 * i;
         c.label.assign((size_t)c.N, (uint8_t)L_WALL);
         c.dlabel = c.label;
         // launch groups: cases of one storage type and collision run in the same kernels
@@ -690,9 +723,7 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
             gi = (int)ctx->groups.size() - 1;
             ctx->groups[gi].dtype = d.dtype;
             ctx->groups[gi].collision = d.collision;
-            if (cudaMalloc(&ctx->groups[gi].d_ints, 4 * sizeof(int)) != cudaSuccess)
-                return set_err(ctx, NNLBM_ERR_OOM, "device allocation failed");
-            cudaMemset(ctx->groups[gi].d_ints, 0, 4 * sizeof(int));
+            ctx->groups[gi].d_ints = (int*)(ctx->d_status + sl.cur) + 4 * gi;
         }
         c.group = gi;
         ctx->groups[gi].cases.push_back(i);
@@ -885,6 +916,7 @@ int nnlbm_init_equilibrium(nnlbm_ctx* ctx, int ic, double rho, double ux, double
     if (c.d_stats) CK(cudaMemsetAsync(c.d_stats, 0, (size_t)6 * c.N * (c.d.stats_f64 ? 8 : 4), ctx->stream));
     CK(cudaMemsetAsync(c.d_err, 0, sizeof(int), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->status_fresh = false;
     c.parity = 0; c.iterations = 0; c.n_stats = 0;
     c.init[0] = rho; c.init[1] = ux; c.init[2] = uy; c.init[3] = uz;
     c.has_state = true;
@@ -952,13 +984,8 @@ int nnlbm_sync(nnlbm_ctx* ctx)
 {
     if (!ctx) return NNLBM_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
-    std::vector<int> err(ctx->cases.size());
-    for (size_t i = 0; i < ctx->cases.size(); ++i)
-        CK(cudaMemcpyAsync(&err[i], ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    for (size_t i = 0; i < ctx->cases.size(); ++i)
-        if (err[i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
-    return NNLBM_OK;
+    const int rc = read_status(ctx);
+    return rc != NNLBM_OK ? rc : check_watchdog(ctx);
 }
 
 int nnlbm_stat_reset(nnlbm_ctx* ctx, int ic)
@@ -1071,7 +1098,9 @@ int nnlbm_reduce(nnlbm_ctx* ctx, int ic, double* out5)
     if (rc) return rc;
     if (!out5) return set_err(ctx, NNLBM_ERR_ARG, "null output");
     CK(cudaSetDevice(ctx->device));
-    CK(cudaMemcpy(out5, ctx->cases[ic].d_red, 5 * sizeof(double), cudaMemcpyDeviceToHost));
+    // a synchronous step has just read the sums back with its cursors and watchdog flags
+    if (!ctx->status_fresh && (rc = read_status(ctx)) != NNLBM_OK) return rc;
+    memcpy(out5, (const double*)(ctx->h_status + StatusLayout(ctx->cases.size()).red) + 8 * ic, 5 * sizeof(double));
     return NNLBM_OK;
 }
 
@@ -1250,7 +1279,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         }
     }
     int cursors[64];
-    int err = 0;
+    ctx->status_fresh = false;
     const size_t n_groups = ctx->groups.size();
     if (n_groups > 64) return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: more than 64 launch groups");
     for (size_t gi = 0; gi < n_groups; ++gi) {
@@ -1295,16 +1324,13 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         if (n_steps < rows) c.sched.erase(c.sched.begin(), c.sched.begin() + 3 * n_steps);
         else c.sched.erase(c.sched.begin(), c.sched.end() - 3);
     }
-    CK(cudaStreamSynchronize(ctx->stream));
+    // the copy of the status block waits for the cursor copies queued before it
+    if ((rc = read_status(ctx)) != NNLBM_OK) return rc;
     for (size_t gi = 0; gi < n_groups; ++gi)
         if (cursors[gi] != n_steps)
             return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", gi, cursors[gi],
                            (long long)n_steps);
-    for (size_t i = 0; i < ctx->cases.size(); ++i) {
-        CK(cudaMemcpy(&err, ctx->cases[i].d_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (err) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
-    }
-    return NNLBM_OK;
+    return check_watchdog(ctx);
 }
 
 void* nnlbm_stream(nnlbm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -1327,15 +1353,17 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
     for (Group& g : ctx->groups) {
         for (int p = 0; p < 2; ++p)
             if (g.graph[p]) cudaGraphExecDestroy(g.graph[p]);
-        void* ptrs[] = {g.d_cases, g.d_chunks, g.d_gather, g.d_nodes, g.d_bc_prof, g.d_bc_buf, g.d_ints};
+        void* ptrs[] = {g.d_cases, g.d_chunks, g.d_gather, g.d_nodes, g.d_bc_prof, g.d_bc_buf};
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }
     for (Case& c : ctx->cases) {
-        void* ptrs[] = {c.df_base, c.d_label, c.d_macro, c.d_stats, c.d_ctl, c.d_red, c.d_err};
+        void* ptrs[] = {c.df_base, c.d_label, c.d_macro, c.d_stats, c.d_ctl};
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NNLBM_OK;
