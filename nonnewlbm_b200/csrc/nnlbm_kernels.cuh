@@ -482,7 +482,8 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// commits the copies issued so far (a wait_group alone skips uncommitted ones) and waits
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // the 32-bit word holding element p (16-bit storage: the aligned pair around it)
 template <class T>
