@@ -208,7 +208,9 @@ int nnlbm_import_df(nnlbm_ctx* ctx, int ic, const double* in);
 
 /* FP64 sums of the last step that had NNLBM_STEP_REDUCE: {mass of FLUID+PERIODIC cells,
  * Q_ivc, Q_svc, Q_outlet5, Q_outlet6}, lattice units, inflow positive at 3/4 and outflow
- * positive at 5/6 (postprocess/compute_flows.py:107-147). */
+ * positive at 5/6 (postprocess/compute_flows.py:107-147).  Right after a synchronous
+ * nnlbm_step (or nnlbm_sync) the sums come from the host copy that call already made of the
+ * context's status words, without another device transfer. */
 int nnlbm_reduce(nnlbm_ctx* ctx, int ic, double* out5);
 
 /* Time the launch shapes of the step kernel on the current state and keep the fastest.

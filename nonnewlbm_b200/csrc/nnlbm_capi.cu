@@ -18,9 +18,7 @@
 #include "nnlbm_kernels.cuh"
 
 namespace nnlbm {
-#define NNLBM_DECL_STEP(DT, COL)                                                        \
-    void launch_step_##DT##_##COL(bool, bool, dim3, dim3, cudaStream_t, const void*); \
-    int prepare_step_##DT##_##COL(int);
+#define NNLBM_DECL_STEP(DT, COL) void launch_step_##DT##_##COL(bool, bool, dim3, dim3, cudaStream_t, const void*);
 #define NNLBM_DECL_STEP_DT(DT)                                                                                        \
     NNLBM_DECL_STEP(DT, 0) NNLBM_DECL_STEP(DT, 1) NNLBM_DECL_STEP(DT, 2) NNLBM_DECL_STEP(DT, 3) NNLBM_DECL_STEP(DT, 4) \
     NNLBM_DECL_STEP(DT, 5) NNLBM_DECL_STEP(DT, 6) NNLBM_DECL_STEP(DT, 7) NNLBM_DECL_STEP(DT, 8) NNLBM_DECL_STEP(DT, 9) \
@@ -41,16 +39,6 @@ StepLauncher step_launcher(int dt, int col)
      launch_step_##DT##_4, launch_step_##DT##_5, launch_step_##DT##_6, launch_step_##DT##_7,             \
      launch_step_##DT##_8, launch_step_##DT##_9, launch_step_##DT##_10}
     static const StepLauncher table[4][11] = {NNLBM_ROW(0), NNLBM_ROW(1), NNLBM_ROW(2), NNLBM_ROW(3)};
-    return table[dt][col];
-}
-
-StepPrep step_prep(int dt, int col)
-{
-#define NNLBM_PREPROW(DT)                                                                                     \
-    {prepare_step_##DT##_0, prepare_step_##DT##_1, prepare_step_##DT##_2, prepare_step_##DT##_3,             \
-     prepare_step_##DT##_4, prepare_step_##DT##_5, prepare_step_##DT##_6, prepare_step_##DT##_7,             \
-     prepare_step_##DT##_8, prepare_step_##DT##_9, prepare_step_##DT##_10}
-    static const StepPrep table[4][11] = {NNLBM_PREPROW(0), NNLBM_PREPROW(1), NNLBM_PREPROW(2), NNLBM_PREPROW(3)};
     return table[dt][col];
 }
 
@@ -144,9 +132,6 @@ struct Group {
     int* d_ints = nullptr;           // the two step cursors (one per A-A parity), in the status block
     bool any_refd = false;
     int block = 256;
-    // the paired step kernel is grid-stride: at most max_blocks blocks of `block` threads
-    // (what the SMs hold at once, set up for prep_block; -1: one warp per work item)
-    int prep_block = 0, max_blocks = -1;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_gen = ~0ull, gen = 0;
     ArgBytes<kGroupArgsBytes> args{}; // GroupArgs<CT>
@@ -165,7 +150,6 @@ struct StatusLayout {
 
 struct nnlbm_ctx {
     int device = 0;
-    int n_sm = 0;
     cudaStream_t stream = nullptr;
     std::vector<Case> cases;
     std::vector<Group> groups;
@@ -378,44 +362,18 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     return NNLBM_OK;
 }
 
-// the step kernel's launch limits for the group's block size (outside any stream capture)
-int prepare_step_grid(nnlbm_ctx* ctx, Group& g)
-{
-    if (g.prep_block == g.block) return NNLBM_OK;
-    const int per_sm = step_prep(g.dtype, g.collision)(g.block);
-    if (per_sm == 0) {
-        cudaGetLastError();
-        return set_err(ctx, NNLBM_ERR_CUDA, "step kernel: no block of %d threads fits an SM", g.block);
-    }
-    g.max_blocks = per_sm < 0 ? -1 : per_sm * ctx->n_sm;
-    g.prep_block = g.block;
-    return NNLBM_OK;
-}
-
 int prepare_group(nnlbm_ctx* ctx, Group& g)
 {
-    if (g.dirty) {
-        const int rc = g.dtype == NNLBM_F64 ? upload_group<double>(ctx, g) : upload_group<float>(ctx, g);
-        if (rc != NNLBM_OK) return rc;
-    }
-    return prepare_step_grid(ctx, g);
+    if (!g.dirty) return NNLBM_OK;
+    return g.dtype == NNLBM_F64 ? upload_group<double>(ctx, g) : upload_group<float>(ctx, g);
 }
 
 // warps of one step launch: one per chunk (per two chunks where the step pairs them),
 // then one per 32 boundary nodes
 int step_warps(const Group& g)
 {
-    const int cw = pairs_chunks(g.dtype, g.collision) ? (g.n_chunks + 1) / 2 : g.n_chunks;
+    const int cw = pairs_chunks(g.dtype, g.collision) ? g.n_chunks / 2 : g.n_chunks;
     return std::max(cw + (int)((g.n_self + 31) / 32), 1);
-}
-
-// grid of one step launch: every work item's warp, or at most the resident grid of a
-// grid-stride variant
-dim3 step_grid(const Group& g)
-{
-    const int per_block = g.block / kChunk;
-    const int n = (step_warps(g) + per_block - 1) / per_block;
-    return dim3(g.max_blocks > 0 ? std::min(n, g.max_blocks) : n);
 }
 
 // enqueue one step of a group (no host synchronisation); `odd` is the A-A parity
@@ -423,7 +381,7 @@ int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
 {
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
-    const dim3 cgrid = step_grid(g), cblk(g.block);
+    const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
     const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
     if (g.any_refd) {
         A.refd_velocity(odd, rgrid, cblk, ctx->stream, g.args.data());
@@ -675,8 +633,7 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
         cudaGetLastError();
         return set_err(ctx, NNLBM_ERR_CUDA, "no CUDA device %d (found %d)", device, ndev);
     }
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
         return set_err(ctx, NNLBM_ERR_CUDA, "cannot initialise device %d", device);
     ctx->cases.resize(n_cases);
     // a group per case at most
@@ -1194,7 +1151,7 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
     if ((rc = prepare_steps(ctx, g, n_steps, flags)) != NNLBM_OK) return rc;
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
-    const dim3 cgrid = step_grid(g), cblk(g.block);
+    const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
     const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
     for (int i = 0; i < 5; ++i) { ms[i] = 0; launches[i] = 0; }
     const int64_t parity = ctx->cases[g.cases[0]].parity;
@@ -1249,11 +1206,10 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
     if (rc != NNLBM_OK) return rc;
     // refuse everything that nnlbm_step would have to allocate, before any launch
     for (size_t gi = 0; gi < ctx->groups.size(); ++gi) {
-        Group& g = ctx->groups[gi];
+        const Group& g = ctx->groups[gi];
         if (g.dirty)
             return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: launch group %zu has no device work list yet; call "
                            "nnlbm_step or nnlbm_step_info once after the map is set", gi);
-        if ((rc = prepare_step_grid(ctx, g)) != NNLBM_OK) return rc;
         const size_t need = (size_t)g.n_self * 4 * (g.dtype == NNLBM_F64 ? 8 : 4);
         if (need > NNLBM_NOALLOC_SCRATCH_BYTES - kNoallocHead)
             return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: launch group %zu has %lld open-plane nodes written by "
@@ -1299,7 +1255,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         else noalloc_args<float>(g, scratch, args);
         const AuxLaunchers& A = aux_launchers(g.dtype);
         const int per_block = g.block / kChunk;
-        const dim3 cgrid = step_grid(g), cblk(g.block);
+        const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
         const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
         const int64_t parity = ctx->cases[g.cases[0]].parity;
         for (int64_t k = 0; k < n_steps; ++k) {

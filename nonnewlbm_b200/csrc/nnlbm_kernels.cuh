@@ -400,10 +400,20 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
 // and the per-cell outputs stay per cell.  A lane whose cell in one chunk does not
 // collide computes that half from the rest state and stores nothing for it.
 // ---------------------------------------------------------------------------------------
+// raw stored value <-> float of the single-precision storage types (no shift, no scale)
 template <int DT> struct Cook;
-template <> struct Cook<1> { __device__ static __forceinline__ float put(float v) { return v; } };
-template <> struct Cook<2> { __device__ static __forceinline__ __half put(float v) { return __float2half_rn(v); } };
-template <> struct Cook<3> { __device__ static __forceinline__ __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); } };
+template <> struct Cook<1> {
+    __device__ static __forceinline__ float put(float v) { return v; }
+    __device__ static __forceinline__ float get(float v) { return v; }
+};
+template <> struct Cook<2> {
+    __device__ static __forceinline__ __half put(float v) { return __float2half_rn(v); }
+    __device__ static __forceinline__ float get(__half v) { return __half2float(v); }
+};
+template <> struct Cook<3> {
+    __device__ static __forceinline__ __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); }
+    __device__ static __forceinline__ float get(__nv_bfloat16 v) { return __bfloat162float(v); }
+};
 
 // the rest of a pair once its populations f (raw stored value + weight, or the rest state
 // where the cell does not collide) are in registers: collision, stores, per-cell outputs
@@ -458,79 +468,20 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Chun
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// the paired step as a software pipeline: while a warp collides one pair, the next pair's
-// populations travel into the warp's staging buffer in shared memory (cp.async, one
-// 32-bit word per value and lane: word [q][h][lane] holds the raw stored value of cell h,
-// zero where that cell does not collide; 16-bit storage copies the aligned word around
-// the value), and the chunk records of the pair after that come in behind them.
-// ---------------------------------------------------------------------------------------
-struct alignas(16) PairStage {
-    uint32_t pop[27 * 64];
-    Chunk rec[3][2]; // a ring of three record pairs
-};
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-// 4 bytes from src, or zeros (nothing read) when !on
-__device__ __forceinline__ void cp_async4(uint32_t* dst, const void* src, bool on)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(on ? 4 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// commits the copies issued so far (a wait_group alone skips uncommitted ones) and waits
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// the 32-bit word holding element p (16-bit storage: the aligned pair around it)
-template <class T>
-__device__ __forceinline__ const void* word_of(const T* p)
-{
-    return sizeof(T) == 4 ? (const void*)p : (const void*)((uintptr_t)p & ~(uintptr_t)3);
-}
-// the value of element p out of its staged word
-template <int DT>
-__device__ __forceinline__ float raw_of(uint32_t wd, const typename Storage<DT>::T* p)
-{
-    if constexpr (DT == 1) {
-        return __uint_as_float(wd);
-    } else {
-        const unsigned short h = (unsigned short)(((uintptr_t)p & 2) ? (wd >> 16) : (wd & 0xffffu));
-        if constexpr (DT == 2) return __half2float(__ushort_as_half(h));
-        else return __bfloat162float(__ushort_as_bfloat16(h));
-    }
-}
-
+// a pair's populations straight from HBM: the raw stored value + weight of each cell, or
+// the rest state where the cell does not collide
 template <int DT, bool ODD>
-__device__ __forceinline__ void stage_pair(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, uint32_t* pop, int lane)
+__device__ __forceinline__ void pair_load(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, int lane, f2* f)
 {
     using T = typename Storage<DT>::T;
     const unsigned bit = 1u << lane;
     const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
     const int cA = ca.c0 + lane, cB = cb.c0 + lane;
-#pragma unroll
-    for (int q = 0; q < 27; ++q) {
-        const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
-        // a cell that does not collide reads nothing (its address may leave the box)
-        cp_async4(pop + q * 64 + lane, fa ? word_of(p + cA) : a.df, fa);
-        cp_async4(pop + q * 64 + 32 + lane, fb ? word_of(p + cB) : a.df, fb);
-    }
-}
-
-template <int DT, bool ODD>
-__device__ __forceinline__ void unstage_pair(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, const uint32_t* pop,
-                                             int lane, f2* f)
-{
-    using T = typename Storage<DT>::T;
-    const int cA = ca.c0 + lane, cB = cb.c0 + lane;
     const f2 isc(a.inv_scale);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
-        const f2 raw(raw_of<DT>(pop[q * 64 + lane], p + cA), raw_of<DT>(pop[q * 64 + 32 + lane], p + cB));
+        const f2 raw(fa ? Cook<DT>::get(p[cA]) : 0.f, fb ? Cook<DT>::get(p[cB]) : 0.f);
         const f2 w(weight<float>(q));
         f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
     }
@@ -579,87 +530,43 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
     }
 }
 
-// a pair that is not pairable, chunk by chunk from direct loads (kept out of line: the
-// pipelined loop's own registers stay free of its needs)
-template <int DT, int COL, bool ODD, bool PARAM>
-__device__ __noinline__ void chunk_by_chunk(const GroupArgs<typename Storage<DT>::CT>& g, const Chunk ca, const Chunk cb,
-                                            int step, int flags, int lane)
-{
-    const int ci = ca.cflags & CH_CASE_MASK, cj = cb.cflags & CH_CASE_MASK;
-    fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[ci] : g.cases[ci], g.cases + ci, ca, step, flags, lane);
-    if (cb.fluid) fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[cj] : g.cases[cj], g.cases + cj, cb, step, flags, lane);
-}
-
-// the step kernel: one warp per chunk of the work list, then one warp per 32 boundary
-// nodes.  Both write only the slots their own cells read, so they run side by side.
-//
-// Paired variants run as a grid-stride loop over pairs (the host launches at most the
-// resident grid) with one PairStage of dynamic shared memory per warp: pair j + W is
-// staged while pair j collides, so only a warp's first pair waits for HBM.  A pair that
-// is not pairable (a face chunk, two cases, the finite-difference force) is stepped
-// chunk by chunk from direct loads, and the warps past the pairs take the node batches.
+// the step kernel: one warp per chunk of the work list (per two chunks where the variant
+// pairs them), then one warp per 32 boundary nodes.  Both write only the slots their own
+// cells read, so they run side by side.
 template <int DT, int COL, bool ODD, bool PARAM>
 __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
     k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
     const int lane = threadIdx.x & 31;
-    int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int step = g.cursor[ODD ? 1 : 0];
     if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
     // the step's flags are the same for every case of the group
     const int flags = (PARAM ? g.cp[0].ctl : g.cases[0].ctl)[step].flags;
     if constexpr (pairs_chunks(DT, COL)) {
-        extern __shared__ PairStage stage_mem[];
-        PairStage& st = stage_mem[threadIdx.x >> 5];
-        const int nw = (int)(gridDim.x * (blockDim.x >> 5));
-        const int np = g.n_chunks >> 1; // the host pads the list to an even length
-        const int nj = np + (g.n_nodes + 31) / 32;
-        // lanes 0-3 copy the 64-byte record pair of pair j into ring slot r
-        auto fetch_records = [&](int j, int r) {
-            if (j < np && lane < 4) cp_async16((char*)st.rec[r] + 16 * lane, (const char*)(g.chunks + 2 * j) + 16 * lane);
-        };
-        auto case_of = [&](const Chunk& c) -> const CaseArgs<CT>& {
-            return PARAM ? g.cp[c.cflags & CH_CASE_MASK] : g.cases[c.cflags & CH_CASE_MASK];
-        };
-        // prologue: the records of the warp's first two pairs, then the first pair's populations
-        fetch_records(w, 0);
-        fetch_records(w + nw, 1);
-        cp_async_wait_all();
-        __syncwarp();
+        // warp w takes chunks 2w and 2w + 1 (the host pads the list to an even length); a
+        // pair that is not pairable (a face chunk, two cases, the finite-difference force)
+        // is stepped chunk by chunk
+        const int np = g.n_chunks >> 1;
         if (w < np) {
-            const Chunk ca = st.rec[0][0], cb = st.rec[0][1];
-            if (pairable<PARAM>(g, ca, cb)) stage_pair<DT, ODD>(case_of(ca), ca, cb, st.pop, lane);
-        }
-        cp_async_commit();
-        // ring slots: r holds this pair's records, r + 1 the next pair's, r + 2 receives the
-        // records of the pair after that
-        int r = 0;
-        for (; w < np; w += nw) {
-            const int wn = w + nw;
-            const int r1 = r == 2 ? 0 : r + 1, r2 = r1 == 2 ? 0 : r1 + 1;
-            // this pair's populations and the next pair's records have landed
-            cp_async_wait_all();
-            __syncwarp();
-            const Chunk ca = st.rec[r][0], cb = st.rec[r][1];
-            const bool staged = pairable<PARAM>(g, ca, cb);
-            const CaseArgs<CT>& a = case_of(ca);
-            f2 f[27];
-            if (staged) unstage_pair<DT, ODD>(a, ca, cb, st.pop, lane, f);
-            __syncwarp(); // every lane holds its words: the population buffer is free
-            if (wn < np) {
-                const Chunk na = st.rec[r1][0], nb = st.rec[r1][1];
-                if (pairable<PARAM>(g, na, nb)) stage_pair<DT, ODD>(case_of(na), na, nb, st.pop, lane);
+            const Chunk ca = g.chunks[2 * w], cb = g.chunks[2 * w + 1];
+            const int ci = ca.cflags & CH_CASE_MASK;
+            const CaseArgs<CT>& a = PARAM ? g.cp[ci] : g.cases[ci];
+            if (pairable<PARAM>(g, ca, cb)) {
+                f2 f[27];
+                pair_load<DT, ODD>(a, ca, cb, lane, f);
+                pair_finish<DT, COL, ODD>(a, ca, cb, f, step, flags, lane);
+            } else {
+                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, step, flags, lane);
+                if (cb.fluid) {
+                    const int cj = cb.cflags & CH_CASE_MASK;
+                    fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[cj] : g.cases[cj], g.cases + cj, cb, step, flags, lane);
+                }
             }
-            fetch_records(wn + nw, r2);
-            cp_async_commit();
-            if (staged) pair_finish<DT, COL, ODD>(a, ca, cb, f, step, flags, lane);
-            else chunk_by_chunk<DT, COL, ODD, PARAM>(g, ca, cb, step, flags, lane);
-            r = r1;
-        }
-        // the node batches follow the pairs
-        for (; w < nj; w += nw)
+        } else {
             node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - np) * 32 + lane, step, flags);
+        }
     } else {
         if (w < g.n_chunks) {
             const Chunk ch = g.chunks[w];
@@ -822,27 +729,18 @@ using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, 
 // gather kernel just enqueued on the stream
 using StepLauncher = void (*)(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 
-// dynamic shared memory of one step-kernel block: a PairStage per warp where the variant
-// pairs its chunks
-template <int DT, int COL>
-constexpr size_t step_smem(unsigned block)
-{
-    return pairs_chunks(DT, COL) ? (size_t)(block / 32) * sizeof(PairStage) : 0;
-}
-
-// launch of one step-kernel variant: one warp per chunk (per pair, grid-stride)
+// launch of one step-kernel variant: one warp per chunk (per pair)
 template <int DT, int COL, bool ODD, bool PARAM>
 void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
-    const size_t smem = step_smem<DT, COL>(block.x);
     if (!after_gather) {
-        k_step<DT, COL, ODD, PARAM><<<grid, block, smem, s>>>(g);
+        k_step<DT, COL, ODD, PARAM><<<grid, block, 0, s>>>(g);
         return;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
+    cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -867,35 +765,6 @@ void launch_step(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_
     }
 }
 
-// set-up of the four step-kernel variants of a (storage, collision) for blocks of `block`
-// threads, outside any stream capture: the dynamic shared memory limit of the paired
-// variants; returns how many such blocks one SM holds (0: none fits), or -1 for variants
-// that are not grid-stride (their grid is one warp per work item)
-template <int DT, int COL, bool ODD, bool PARAM>
-int prepare_step_variant(int block)
-{
-    const size_t smem = step_smem<DT, COL>((unsigned)block);
-    if (cudaFuncSetAttribute(k_step<DT, COL, ODD, PARAM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-        return 0;
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<DT, COL, ODD, PARAM>, block, smem) != cudaSuccess) return 0;
-    return n;
-}
-template <int DT, int COL>
-int prepare_step(int block)
-{
-    if constexpr (!pairs_chunks(DT, COL)) {
-        return -1;
-    } else {
-        const int n[4] = {prepare_step_variant<DT, COL, false, false>(block), prepare_step_variant<DT, COL, false, true>(block),
-                          prepare_step_variant<DT, COL, true, false>(block), prepare_step_variant<DT, COL, true, true>(block)};
-        return std::min(std::min(n[0], n[1]), std::min(n[2], n[3]));
-    }
-}
-using StepPrep = int (*)(int block);
-
 StepLauncher step_launcher(int dtype, int collision);
-StepPrep step_prep(int dtype, int collision);
 
 } // namespace nnlbm

@@ -19,5 +19,4 @@ void NNLBM_CAT(launch_step_, NNLBM_DT, NNLBM_COL)(bool odd, bool after_gather, d
 {
     launch_step<NNLBM_DT, NNLBM_COL>(odd, after_gather, grid, block, s, args);
 }
-int NNLBM_CAT(prepare_step_, NNLBM_DT, NNLBM_COL)(int block) { return prepare_step<NNLBM_DT, NNLBM_COL>(block); }
 } // namespace nnlbm
