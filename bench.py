@@ -395,24 +395,25 @@ def run_ours(a, dist: Dist) -> int:
     traffic = ncu_traffic(key)
 
     # end to end through the public API: per step the host sends that step's inflow row
-    # and reads back the FP64 mass / flux sums
+    # (a +-1 % pulsation, so every row differs from the last and is uploaded) and reads
+    # back the FP64 mass / flux sums
     if w.kind == "tcpc":
-        rows = np.array([[w.u_ivc * w.notes["counts"]["left_area"], w.u_svc * w.notes["counts"]["right_area"], 1.0]])
+        q0 = np.array([w.u_ivc * w.notes["counts"]["left_area"], w.u_svc * w.notes["counts"]["right_area"]])
     else:
-        rows = np.array([[0.0, 0.0, 1.0]])
+        q0 = np.zeros(2)
+    rows = [np.array([[*(q0 * (1.0 + 0.01 * np.sin(0.1 * k))), 1.0]]) for k in range(a.e2e_steps)]
     dist.barrier()
     t0 = time.perf_counter()
     red = None
-    for _ in range(a.e2e_steps):
-        lat.set_schedule(rows)
+    for k in range(a.e2e_steps):
+        lat.set_schedule(rows[k])
         lat.step(1, stats=stats, reduce=True)
         red = lat.reduce()
     t_e2e = time.perf_counter() - t0
     t_e2e = dist.max(t_e2e)
     e2e = fluid * a.e2e_steps * dist.world / t_e2e / 1e6
-    ctl_bytes = 32 if w.dtype != "f64" else 56
-    h2d = ctl_bytes + 8  # the step's control row + the cursor reset
-    d2h = 5 * 8 + 3 * 4  # mass/flux sums + the watchdog / cursor words
+    h2d = 32 if w.dtype != "f64" else 56  # the step's control row
+    d2h = 88  # the context's status block: step cursors, watchdog flag, mass/flux sums
     lat.close()
 
     if dist.rank == 0:
