@@ -168,6 +168,21 @@ def test_reduced_precision_vs_fp64_oracle(dtype, tol_u):
         assert err <= tol_u, (dtype, err)
 
 
+@pytest.mark.parametrize("collision", [9, 10, 4, 5], ids=["MRT_LES", "BGK", "KBC_N4", "KBC_C1"])
+def test_fp32_collisions_vs_fp64_oracle(collision):
+    """FP32 storage and arithmetic of the other collisions against the FP64 oracle after 200
+    steps (MRT and BGK run two cells per thread on the packed FP32 pipe, KBC one), relative to
+    the peak velocity."""
+    orc, lat = _tcpc_pair(collision, dtype="f32")
+    orc.step(200)
+    lat.step(200, macro=True)
+    fluid = orc.get_map() == G.MAP_FLUID
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
+    for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
+        assert err <= 2e-5, (O.COLLISIONS[collision], err)
+
+
 def test_autotune_keeps_state():
     orc, lat = _tcpc_pair(0)
     orc.step(4)
