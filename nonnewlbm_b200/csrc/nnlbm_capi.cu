@@ -63,14 +63,14 @@ namespace {
 
 const int kStorageBytes[4] = {8, 4, 2, 2};
 const int kChunk = 32;
-// slack around the populations and after the labels: the staged rows of a chunk start at
-// the 16-byte boundary at or below the first element and end up to 16 bytes past the
-// chunk, which at the ends of the arrays reaches outside them
+// slack around the populations and after the labels: every kernel reads only cells of the
+// box, so nothing is read here; the slack keeps each allocation's start and end away from
+// the first and last 32-cell row
 const size_t kDfPad = 512;
 const size_t kLabelPad = 64;
 
-// storage for the kernel arguments of either arithmetic type: they hold 64-byte aligned
-// tensor maps, so the bytes are aligned like the structures they stand for
+// storage for the kernel arguments of either arithmetic type, aligned like the structures
+// they stand for
 template <size_t N>
 struct alignas(64) ArgBytes {
     unsigned char bytes[N];
@@ -141,11 +141,12 @@ struct Group {
 
 // every word the host reads back after a step, in one device block (and one pinned host
 // mirror) so that a synchronous step costs one small copy: per launch group 4 ints (the
-// two step cursors), per case 2 ints (the watchdog flag) and 8 doubles (the reductions)
+// two step cursors), per case 8 doubles (the reductions) and 2 ints (the watchdog flag).
+// The cursors and the sums lead, so that one memset clears what a step call restarts.
 struct StatusLayout {
-    size_t cur, err, red, bytes;
+    size_t cur, red, err, bytes;
     explicit StatusLayout(size_t n_slots)
-        : cur(0), err(16 * n_slots), red(24 * n_slots), bytes(88 * n_slots) {}
+        : cur(0), red(16 * n_slots), err(80 * n_slots), bytes(88 * n_slots) {}
 };
 
 struct nnlbm_ctx {
@@ -413,7 +414,9 @@ int ensure_graphs(nnlbm_ctx* ctx, Group& g)
 }
 
 // host side of one nnlbm_step call for every case of a group, up to the launches
-int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags)
+// `reset`: clear the group's step cursors (and its cases' sums for NNLBM_STEP_REDUCE); a
+// caller that cleared the whole status block already passes false
+int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = true)
 {
     int rc;
     int64_t parity = -1;
@@ -438,10 +441,10 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags)
             CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
             c.ctl_dev = buf;
         }
-        if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
+        if (reset && (flags & NNLBM_STEP_REDUCE)) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
     }
     if ((rc = prepare_group(ctx, g)) != NNLBM_OK) return rc;
-    CK(cudaMemsetAsync(g.d_ints, 0, 2 * sizeof(int), ctx->stream));
+    if (reset) CK(cudaMemsetAsync(g.d_ints, 0, 2 * sizeof(int), ctx->stream));
     return NNLBM_OK;
 }
 
@@ -455,9 +458,9 @@ void finish_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags)
     }
 }
 
-int run_group_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool use_graph)
+int run_group_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool use_graph, bool reset = true)
 {
-    int rc = prepare_steps(ctx, g, n, flags);
+    int rc = prepare_steps(ctx, g, n, flags, reset);
     if (rc) return rc;
     if (use_graph && (rc = ensure_graphs(ctx, g)) != NNLBM_OK) return rc;
     const int64_t parity = ctx->cases[g.cases[0]].parity;
@@ -922,8 +925,11 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
     if (n_steps < 0) return set_err(ctx, NNLBM_ERR_ARG, "negative step count");
     if (n_steps == 0) return NNLBM_OK;
     CK(cudaSetDevice(ctx->device));
+    // one memset restarts every group's step cursors (and, for a reduction, every case's sums)
+    const StatusLayout sl(ctx->cases.size());
+    CK(cudaMemsetAsync(ctx->d_status, 0, (flags & NNLBM_STEP_REDUCE) ? sl.err : sl.red, ctx->stream));
     for (Group& g : ctx->groups) {
-        int rc = run_group_steps(ctx, g, n_steps, flags, true);
+        int rc = run_group_steps(ctx, g, n_steps, flags, true, false);
         if (rc != NNLBM_OK) return rc;
     }
     for (Case& c : ctx->cases) {
