@@ -230,7 +230,8 @@ def run_reference(a, dist: Dist):
     threads = os.cpu_count() or 1
     O.ref_lib(fast=True).ref_set_threads(threads)
     ref, fluid, what = reference_lattice(w, a.collision)
-    warm = max(1, min(a.warmup, 2))
+    # at least 3 warm-up steps like the GPU arm, at most 5 (a reference step takes ~0.2 s)
+    warm = min(max(a.warmup, 3), 5)
     for _ in range(warm):
         ref.step(1, accumulate_stats=not a.no_stats)
     times = []
