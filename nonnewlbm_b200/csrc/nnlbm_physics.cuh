@@ -529,17 +529,40 @@ __device__ __forceinline__ CT cy_nu_from_central(CT Cxx, CT Cyy, CT Czz, CT Cxy,
     return (tau - CT(0.5)) * CT(1.0 / 3.0);
 }
 
-// two cells at once: the Newton solve runs per half (its branches and transcendental
-// functions are scalar)
+// two cells at once: the same Newton solve in packed arithmetic; the powers, square roots
+// and divisions run per half, and a half whose strain is zero keeps tau = 3 nu0 + 1/2
 __device__ __forceinline__ f2 cy_nu_from_central(f2 Cxx, f2 Cyy, f2 Czz, f2 Cxy, f2 Cxz, f2 Cyz, f2 rho,
                                                  const CYParams<float>& p, f2* S)
 {
-    float Sa[6], Sb[6];
-    const float na = cy_nu_from_central<float>(Cxx.v.x, Cyy.v.x, Czz.v.x, Cxy.v.x, Cxz.v.x, Cyz.v.x, rho.v.x, p, Sa);
-    const float nb = cy_nu_from_central<float>(Cxx.v.y, Cyy.v.y, Czz.v.y, Cxy.v.y, Cxz.v.y, Cyz.v.y, rho.v.y, p, Sb);
+    const f2 third(1.0 / 3.0), half(0.5), three(3.0), one(1.0);
+    const f2 Pxx = Cxx - rho * third, Pyy = Cyy - rho * third, Pzz = Czz - rho * third;
+    const f2 pn = dsqrt<f2>(Pxx * Pxx + Pyy * Pyy + Pzz * Pzz + f2(2.0) * (Cxy * Cxy + Cxz * Cxz + Cyz * Cyz));
+    const f2 K = three * f2(1.4142135623730951) * pn / (f2(2.0) * rho);
+    const f2 tau0 = three * f2(p.nu0) + half;
+    f2 tau = tau0;
+    const bool ka = K.v.x > 0.f, kb = K.v.y > 0.f;
+    if (ka || kb) {
+        const float e = (p.n - 1.f) / p.a;
+        const f2 dn(p.nu0 - p.nu_inf), ninf(p.nu_inf), lam(p.lam), nm1(p.n - 1.f);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) S[k] = f2(Sa[k], Sb[k]);
-    return f2(na, nb);
+        for (int it = 0; it < 3; ++it) {
+            const f2 g = K / tau;
+            const f2 lg = lam * g;
+            // (lambda gamma)^a; the usual a = 2 is a product
+            const f2 s = p.a == 2.f ? lg * lg : f2(dpow<float>(lg.v.x, p.a), dpow<float>(lg.v.y, p.a));
+            const f2 s1 = one + s;
+            const f2 pw(dpow<float>(s1.v.x, e), dpow<float>(s1.v.y, e));
+            const f2 nuc = ninf + dn * pw;
+            const f2 G = tau - three * nuc - half;
+            const f2 gdn = dn * nm1 * s * pw / s1;
+            const f2 Gp = one + three * gdn / tau;
+            tau = tau - G / Gp;
+        }
+        tau = f2(ka ? tau.v.x : tau0.v.x, kb ? tau.v.y : tau0.v.y);
+    }
+    const f2 sc = f2(-3.0) / (f2(2.0) * rho * tau);
+    S[0] = sc * Pxx; S[1] = sc * Cxy; S[2] = sc * Cxz; S[3] = sc * Pyy; S[4] = sc * Cyz; S[5] = sc * Pzz;
+    return (tau - half) * third;
 }
 
 // the same from the populations: raw second moments by additions only (c in {-1,0,1}),

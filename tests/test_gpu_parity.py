@@ -183,6 +183,23 @@ def test_fp32_collisions_vs_fp64_oracle(collision):
         assert err <= 2e-5, (O.COLLISIONS[collision], err)
 
 
+@pytest.mark.parametrize("dtype,tol_u", [("f32", 5e-5), ("f16", 2e-3)])
+def test_reduced_precision_cy_local_neq(dtype, tol_u):
+    """The cumulant with the local Carreau-Yasuda viscosity (solved two cells at a time in
+    packed single precision) against the FP64 oracle after 200 steps, relative to the peak
+    velocity; the viscosity field itself within 1e-3 of its largest value."""
+    orc, lat = _tcpc_pair(0, dtype=dtype, cy_mode=O.CY_LOCAL_NEQ, cy=CY)
+    orc.step(200)
+    lat.step(200, macro=True)
+    fluid = orc.get_map() == G.MAP_FLUID
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
+    for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
+        assert err <= tol_u, (dtype, err)
+    s_o, s_l = orc.get_macro(O.M_S12)[fluid], lat.macro(capi.M_S12)[fluid]
+    assert np.max(np.abs(s_l - s_o)) <= 1e-3 * np.max(np.abs(s_o)), dtype
+
+
 def test_autotune_keeps_state():
     orc, lat = _tcpc_pair(0)
     orc.step(4)
