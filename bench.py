@@ -353,7 +353,7 @@ def storage_comparison(a, flush: L2Flush, dev: int, f32_mlups: float) -> dict:
     w = workload(a, "f16")
     lat = W.build_lattice(w, device=dev)
     fluid = lat.step_info()["fluid_cells"]
-    lat.autotune()
+    lat.autotune(stats=not a.no_stats)
     lat.step(max(3, a.warmup), stats=not a.no_stats)
     n = max(20, min(a.steps, 200))
     ms = timed_steps(lat, n, not a.no_stats, flush, dev)
@@ -388,7 +388,7 @@ def run_ours(a, dist: Dist) -> int:
     w = workload(a)
     lat = W.build_lattice(w, device=dev)
     info = lat.step_info()
-    lat.autotune()
+    lat.autotune(stats=stats)
     lat.step(max(3, a.warmup), stats=stats)
     # the populations touched per step can be smaller than the 126 MB L2 (a sparse
     # junction), so every timed step starts from a cold L2

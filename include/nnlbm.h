@@ -213,9 +213,17 @@ int nnlbm_import_df(nnlbm_ctx* ctx, int ic, const double* in);
  * context's status words, without another device transfer. */
 int nnlbm_reduce(nnlbm_ctx* ctx, int ic, double* out5);
 
-/* Time the launch shapes of the step kernel on the current state and keep the fastest.
+/* Time the launch shapes of the step kernel on copies of the current state and keep the
+ * fastest: the block size, and for the single-precision cumulant, BGK and MRT whether a
+ * thread steps two cells (packed FP32) or one.  The two forms round differently, so
+ * contexts that must agree bitwise should share the form (the default is two cells).
  * No reference counterpart (the reference takes --block-size, sim_tcpc.cu:118-119). */
 int nnlbm_autotune(nnlbm_ctx* ctx);
+
+/* nnlbm_autotune timing steps that carry `flags` (NNLBM_STEP_STATS, NNLBM_STEP_MACRO; the
+ * others are ignored), for a caller that will step with them; the mean/rms sums and macro
+ * fields are restored afterwards like the populations. */
+int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags);
 
 /* Number of populations-kernel launches and bytes moved per step for case ic
  * (roofline bookkeeping). */

@@ -27,7 +27,7 @@ M_RHO, M_VX, M_VY, M_VZ, M_FX, M_FY, M_FZ, M_S11, M_S12, M_S13, M_S22, M_S32, M_
 EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
     "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_step_noalloc", "nnlbm_stat_reset", "nnlbm_get_macro",
-    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_step_info", "nnlbm_profile_step",
+    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_step_info", "nnlbm_profile_step",
     "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels", "nnlbm_sync",
 ]
 
@@ -79,6 +79,7 @@ def lib():
         L.nnlbm_import_df.argtypes = [_vp, i, _dp]
         L.nnlbm_reduce.argtypes = [_vp, i, _dp]
         L.nnlbm_autotune.argtypes = [_vp]
+        L.nnlbm_autotune_flags.argtypes = [_vp, i]
         L.nnlbm_step_info.argtypes = [_vp, i, _i64p, _i64p, _i64p, _dp]
         L.nnlbm_profile_step.argtypes = [_vp, i, ctypes.c_int64, i, _dp, _i64p]
         L.nnlbm_sync.argtypes = [_vp]

@@ -18,7 +18,7 @@
 #include "nnlbm_kernels.cuh"
 
 namespace nnlbm {
-#define NNLBM_DECL_STEP(DT, COL) void launch_step_##DT##_##COL(bool, bool, dim3, dim3, cudaStream_t, const void*);
+#define NNLBM_DECL_STEP(DT, COL) void launch_step_##DT##_##COL(bool, bool, bool, dim3, dim3, cudaStream_t, const void*);
 #define NNLBM_DECL_STEP_DT(DT)                                                                                        \
     NNLBM_DECL_STEP(DT, 0) NNLBM_DECL_STEP(DT, 1) NNLBM_DECL_STEP(DT, 2) NNLBM_DECL_STEP(DT, 3) NNLBM_DECL_STEP(DT, 4) \
     NNLBM_DECL_STEP(DT, 5) NNLBM_DECL_STEP(DT, 6) NNLBM_DECL_STEP(DT, 7) NNLBM_DECL_STEP(DT, 8) NNLBM_DECL_STEP(DT, 9) \
@@ -132,6 +132,7 @@ struct Group {
     int* d_ints = nullptr;           // the two step cursors (one per A-A parity), in the status block
     bool any_refd = false;
     int block = 256;
+    bool paired = false;             // two cells a thread (set where the collision can pair)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_gen = ~0ull, gen = 0;
     ArgBytes<kGroupArgsBytes> args{}; // GroupArgs<CT>
@@ -373,7 +374,7 @@ int prepare_group(nnlbm_ctx* ctx, Group& g)
 // then one per 32 boundary nodes
 int step_warps(const Group& g)
 {
-    const int cw = pairs_chunks(g.dtype, g.collision) ? g.n_chunks / 2 : g.n_chunks;
+    const int cw = g.paired ? g.n_chunks / 2 : g.n_chunks;
     return std::max(cw + (int)((g.n_self + 31) / 32), 1);
 }
 
@@ -389,7 +390,7 @@ int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
         A.refd_stress(odd, rgrid, cblk, ctx->stream, g.args.data());
     }
     if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
-    step_launcher(g.dtype, g.collision)(odd, g.n_gather > 0, cgrid, cblk, ctx->stream, g.args.data());
+    step_launcher(g.dtype, g.collision)(odd, g.n_gather > 0, g.paired, cgrid, cblk, ctx->stream, g.args.data());
     CK(cudaGetLastError());
     return NNLBM_OK;
 }
@@ -683,6 +684,7 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
             gi = (int)ctx->groups.size() - 1;
             ctx->groups[gi].dtype = d.dtype;
             ctx->groups[gi].collision = d.collision;
+            ctx->groups[gi].paired = pairs_chunks(d.dtype, d.collision);
             ctx->groups[gi].d_ints = (int*)(ctx->d_status + sl.cur) + 4 * gi;
         }
         c.group = gi;
@@ -1067,19 +1069,25 @@ int nnlbm_reduce(nnlbm_ctx* ctx, int ic, double* out5)
     return NNLBM_OK;
 }
 
-int nnlbm_autotune(nnlbm_ctx* ctx)
+int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags)
 {
     if (!ctx) return NNLBM_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
     static const int blocks[] = {64, 128, 256};
+    const int tf = flags & (NNLBM_STEP_STATS | NNLBM_STEP_MACRO);
     for (Group& g : ctx->groups) {
         bool ready = true;
         for (int ic : g.cases) ready = ready && ctx->cases[ic].has_map && ctx->cases[ic].has_state;
         if (!ready) continue;
-        // tune on copies of the states so that the lattices do not advance
-        std::vector<void*> saved, msaved;
+        int rc;
+        // tune on copies of the states (populations, macro fields, mean/rms sums) so that the
+        // lattices do not advance
+        std::vector<void*> saved, msaved, ssaved;
+        std::vector<int64_t> par, it, nst;
         for (int ic : g.cases) {
             Case& c = ctx->cases[ic];
+            if ((tf & NNLBM_STEP_MACRO) && (rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
+            if ((tf & NNLBM_STEP_STATS) && (rc = ensure_stats(ctx, c)) != NNLBM_OK) return rc;
             const size_t bytes = 27 * c.q_stride * kStorageBytes[c.d.dtype];
             void* p = nullptr;
             CK(cudaMalloc(&p, bytes));
@@ -1092,44 +1100,62 @@ int nnlbm_autotune(nnlbm_ctx* ctx)
                 CK(cudaMemcpyAsync(m, c.d_macro, mb, cudaMemcpyDeviceToDevice, ctx->stream));
             }
             msaved.push_back(m);
+            void* st = nullptr;
+            if (c.d_stats && (tf & NNLBM_STEP_STATS)) {
+                const size_t sb = (size_t)6 * c.N * (c.d.stats_f64 ? 8 : 4);
+                CK(cudaMalloc(&st, sb));
+                CK(cudaMemcpyAsync(st, c.d_stats, sb, cudaMemcpyDeviceToDevice, ctx->stream));
+            }
+            ssaved.push_back(st);
+            par.push_back(c.parity); it.push_back(c.iterations); nst.push_back(c.n_stats);
         }
-        std::vector<int64_t> par, it;
-        for (int ic : g.cases) { par.push_back(ctx->cases[ic].parity); it.push_back(ctx->cases[ic].iterations); }
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
+        // every launch shape: block size x (where the collision pairs) one or two cells a thread
         float best = 1e30f;
         int bb = g.block;
-        for (int b : blocks) {
-            g.block = b;
-            int rc = run_group_steps(ctx, g, 2, 0, false);
-            if (rc) return rc;
-            CK(cudaEventRecord(e0, ctx->stream));
-            rc = run_group_steps(ctx, g, 6, 0, false);
-            if (rc) return rc;
-            CK(cudaEventRecord(e1, ctx->stream));
-            CK(cudaEventSynchronize(e1));
-            float ms = 0;
-            CK(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) { best = ms; bb = b; }
+        bool bp = g.paired;
+        const int n_forms = pairs_chunks(g.dtype, g.collision) ? 2 : 1;
+        for (int form = 0; form < n_forms; ++form) {
+            for (int b : blocks) {
+                g.block = b;
+                g.paired = n_forms == 2 && form == 0;
+                if ((rc = run_group_steps(ctx, g, 3, tf, false)) != NNLBM_OK) return rc;
+                CK(cudaEventRecord(e0, ctx->stream));
+                if ((rc = run_group_steps(ctx, g, 10, tf, false)) != NNLBM_OK) return rc;
+                CK(cudaEventRecord(e1, ctx->stream));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) { best = ms; bb = b; bp = g.paired; }
+            }
         }
         g.block = bb;
+        g.paired = bp;
         g.gen++; // the graphs captured another launch shape
         for (size_t j = 0; j < g.cases.size(); ++j) {
             Case& c = ctx->cases[g.cases[j]];
-            c.parity = par[j]; c.iterations = it[j];
+            c.parity = par[j]; c.iterations = it[j]; c.n_stats = nst[j];
             CK(cudaMemcpyAsync(c.df, saved[j], 27 * c.q_stride * kStorageBytes[c.d.dtype], cudaMemcpyDeviceToDevice, ctx->stream));
             if (msaved[j]) CK(cudaMemcpyAsync(c.d_macro, msaved[j], (size_t)M_N * c.N * c.ct_bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+            if (ssaved[j])
+                CK(cudaMemcpyAsync(c.d_stats, ssaved[j], (size_t)6 * c.N * (c.d.stats_f64 ? 8 : 4), cudaMemcpyDeviceToDevice,
+                                   ctx->stream));
         }
         CK(cudaStreamSynchronize(ctx->stream));
         for (void* p : saved) cudaFree(p);
         for (void* p : msaved)
+            if (p) cudaFree(p);
+        for (void* p : ssaved)
             if (p) cudaFree(p);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
     return NNLBM_OK;
 }
+
+int nnlbm_autotune(nnlbm_ctx* ctx) { return nnlbm_autotune_flags(ctx, 0); }
 
 int nnlbm_step_info(nnlbm_ctx* ctx, int ic, int64_t* fluid_cells, int64_t* bc_cells, int64_t* launches_per_step,
                     double* bytes_per_step)
@@ -1184,7 +1210,7 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
             A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
             mark(0);
         }
-        step_launcher(g.dtype, g.collision)(odd, false, cgrid, cblk, ctx->stream, g.args.data());
+        step_launcher(g.dtype, g.collision)(odd, false, g.paired, cgrid, cblk, ctx->stream, g.args.data());
         mark(1);
         CK(cudaGetLastError());
     }
@@ -1271,7 +1297,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
                 A.refd_stress(odd, rgrid, cblk, ctx->stream, args);
             }
             if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, args);
-            step_launcher(g.dtype, g.collision)(odd, false, cgrid, cblk, ctx->stream, args);
+            step_launcher(g.dtype, g.collision)(odd, false, g.paired, cgrid, cblk, ctx->stream, args);
         }
         CK(cudaGetLastError());
         // pageable destination: the copy returns once the cursor is on the host; the last

@@ -296,14 +296,18 @@ __host__ __device__ constexpr bool pairs_chunks(int dt, int col)
 }
 
 // register budget per thread of each step-kernel variant: FP64 arithmetic may use all
-// 255; the paired variants (two cells per thread) get NNLBM_PAIR_REGS; everything else
-// 128, two 256-thread blocks per SM
+// 255; the paired form (two cells per thread) gets NNLBM_PAIR_REGS (two 256-thread blocks
+// per SM); the one-cell form of a collision that can pair gets NNLBM_CHUNK_REGS (four
+// blocks); KBC, which never pairs, 128
 #ifndef NNLBM_PAIR_REGS
 #define NNLBM_PAIR_REGS 128
 #endif
-template <int DT, int COL>
+#ifndef NNLBM_CHUNK_REGS
+#define NNLBM_CHUNK_REGS 64
+#endif
+template <int DT, int COL, bool PAIR>
 struct StepRegs {
-    static constexpr int value = DT == 0 ? 255 : pairs_chunks(DT, COL) ? NNLBM_PAIR_REGS : 128;
+    static constexpr int value = DT == 0 ? 255 : !pairs_chunks(DT, COL) ? 128 : PAIR ? NNLBM_PAIR_REGS : NNLBM_CHUNK_REGS;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -533,8 +537,8 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
 // the step kernel: one warp per chunk of the work list (per two chunks where the variant
 // pairs them), then one warp per 32 boundary nodes.  Both write only the slots their own
 // cells read, so they run side by side.
-template <int DT, int COL, bool ODD, bool PARAM>
-__global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
+template <int DT, int COL, bool ODD, bool PARAM, bool PAIR>
+__global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::value))
     k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
@@ -544,7 +548,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL>::value))
     if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
     // the step's flags are the same for every case of the group
     const int flags = (PARAM ? g.cp[0].ctl : g.cases[0].ctl)[step].flags;
-    if constexpr (pairs_chunks(DT, COL)) {
+    if constexpr (PAIR && pairs_chunks(DT, COL)) {
         // warp w takes chunks 2w and 2w + 1 (the host pads the list to an even length); a
         // pair that is not pairable (a face chunk, two cases, the finite-difference force)
         // is stepped chunk by chunk
@@ -726,15 +730,16 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
 // ---------------------------------------------------------------------------------------
 using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
 // the step kernel's launcher: `after_gather` launches it as a programmatic dependent of the
-// gather kernel just enqueued on the stream
-using StepLauncher = void (*)(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
+// gather kernel just enqueued on the stream; `paired` picks the two-cells-per-thread form
+using StepLauncher = void (*)(bool odd, bool after_gather, bool paired, dim3 grid, dim3 block, cudaStream_t s,
+                              const void* group_args);
 
 // launch of one step-kernel variant: one warp per chunk (per pair)
-template <int DT, int COL, bool ODD, bool PARAM>
+template <int DT, int COL, bool ODD, bool PARAM, bool PAIR>
 void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
     if (!after_gather) {
-        k_step<DT, COL, ODD, PARAM><<<grid, block, 0, s>>>(g);
+        k_step<DT, COL, ODD, PARAM, PAIR><<<grid, block, 0, s>>>(g);
         return;
     }
     cudaLaunchConfig_t cfg = {};
@@ -747,22 +752,35 @@ void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t 
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_step<DT, COL, ODD, PARAM>, g);
+    cudaLaunchKernelEx(&cfg, k_step<DT, COL, ODD, PARAM, PAIR>, g);
 }
 
+template <int DT, int COL, bool PAIR>
+void launch_step_form(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
+{
+    // PARAM: the cases' arguments are in parameter space (g.cp)
+    if (g.n_cases <= kParamCases) {
+        if (odd) launch_step_variant<DT, COL, true, true, PAIR>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, true, PAIR>(after_gather, grid, block, s, g);
+    } else {
+        if (odd) launch_step_variant<DT, COL, true, false, PAIR>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, false, PAIR>(after_gather, grid, block, s, g);
+    }
+}
+
+// `paired`: the two-cells-per-thread form where the collision has one (pairs_chunks)
 template <int DT, int COL>
-void launch_step(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const void* args)
+void launch_step(bool odd, bool after_gather, bool paired, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
-    // PARAM: the cases' arguments are in parameter space (g.cp)
-    if (g.n_cases <= kParamCases) {
-        if (odd) launch_step_variant<DT, COL, true, true>(after_gather, grid, block, s, g);
-        else launch_step_variant<DT, COL, false, true>(after_gather, grid, block, s, g);
-    } else {
-        if (odd) launch_step_variant<DT, COL, true, false>(after_gather, grid, block, s, g);
-        else launch_step_variant<DT, COL, false, false>(after_gather, grid, block, s, g);
+    if constexpr (pairs_chunks(DT, COL)) {
+        if (paired) {
+            launch_step_form<DT, COL, true>(odd, after_gather, grid, block, s, g);
+            return;
+        }
     }
+    launch_step_form<DT, COL, false>(odd, after_gather, grid, block, s, g);
 }
 
 StepLauncher step_launcher(int dtype, int collision);

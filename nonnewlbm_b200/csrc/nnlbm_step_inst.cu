@@ -14,9 +14,9 @@
 #define NNLBM_CAT(a, b, c) NNLBM_CAT2(a, b, c)
 
 namespace nnlbm {
-void NNLBM_CAT(launch_step_, NNLBM_DT, NNLBM_COL)(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s,
-                                                const void* args)
+void NNLBM_CAT(launch_step_, NNLBM_DT, NNLBM_COL)(bool odd, bool after_gather, bool paired, dim3 grid, dim3 block,
+                                                cudaStream_t s, const void* args)
 {
-    launch_step<NNLBM_DT, NNLBM_COL>(odd, after_gather, grid, block, s, args);
+    launch_step<NNLBM_DT, NNLBM_COL>(odd, after_gather, paired, grid, block, s, args);
 }
 } // namespace nnlbm

@@ -132,8 +132,10 @@ class Lattice:
         flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0) | (capi.STEP_REDUCE if reduce else 0)
         self._chk(capi.lib().nnlbm_step_noalloc(self.h, int(n), flags))
 
-    def autotune(self) -> None:
-        self._chk(capi.lib().nnlbm_autotune(self.h))
+    def autotune(self, stats: bool = False, macro: bool = False) -> None:
+        """Pick the fastest step-kernel launch shape, timing steps with these flags."""
+        flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0)
+        self._chk(capi.lib().nnlbm_autotune_flags(self.h, flags))
 
     def stat_reset(self, ic: int | None = None) -> None:
         for k in self._cases(ic):

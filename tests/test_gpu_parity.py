@@ -210,6 +210,25 @@ def test_autotune_keeps_state():
     assert max_rel(lat.export_df(), orc.get_df(), dead_mask(orc.get_map())) <= FP64_TOL
 
 
+def test_autotune_with_stats_restores_state():
+    """Tuning with the accumulators on (which may switch an FP32 cumulant between one and two
+    cells a thread) leaves populations, mean/rms sums and their step count as they were."""
+    orc, lat = _tcpc_pair(0, dtype="f32", cy_mode=O.CY_LOCAL_NEQ, cy=CY)
+    lat.step(10, stats=True)
+    df0, (st0, n0) = lat.export_df(), lat.stats()
+    lat.autotune(stats=True)
+    st1, n1 = lat.stats()
+    assert np.array_equal(lat.export_df(), df0) and np.array_equal(st1, st0) and n1 == n0 == 10
+    # the tuned form steps on correctly
+    lat.step(10, stats=True, macro=True)
+    assert lat.stats()[1] == 20
+    orc.step(20)
+    fluid = orc.get_map() == G.MAP_FLUID
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
+    err = np.max(np.abs(lat.macro(capi.M_VX)[fluid] - orc.get_macro(O.M_VX)[fluid])) / umax
+    assert err <= 5e-5, err
+
+
 def test_batched_cases_match_single():
     wall = small_junction()
     nz, ny, nx = wall.shape
