@@ -54,12 +54,18 @@ void NNLBM_CAT(launch_bc_gather_, NNLBM_DT)(bool odd, dim3 grid, dim3 block, cud
 {
     using CT = typename Storage<NNLBM_DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
-    if (g.n_cases <= kParamCases) {
-        if (odd) k_bc_gather<NNLBM_DT, true, true><<<grid, block, 0, s>>>(g);
-        else k_bc_gather<NNLBM_DT, false, true><<<grid, block, 0, s>>>(g);
-    } else {
-        if (odd) k_bc_gather<NNLBM_DT, true, false><<<grid, block, 0, s>>>(g);
-        else k_bc_gather<NNLBM_DT, false, false><<<grid, block, 0, s>>>(g);
+    switch (args_mode(g.n_cases)) {
+    case ARGS_ONE:
+        if (odd) k_bc_gather<NNLBM_DT, true, ARGS_ONE><<<grid, block, 0, s>>>(g);
+        else k_bc_gather<NNLBM_DT, false, ARGS_ONE><<<grid, block, 0, s>>>(g);
+        break;
+    case ARGS_PARAM:
+        if (odd) k_bc_gather<NNLBM_DT, true, ARGS_PARAM><<<grid, block, 0, s>>>(g);
+        else k_bc_gather<NNLBM_DT, false, ARGS_PARAM><<<grid, block, 0, s>>>(g);
+        break;
+    default:
+        if (odd) k_bc_gather<NNLBM_DT, true, ARGS_GLOBAL><<<grid, block, 0, s>>>(g);
+        else k_bc_gather<NNLBM_DT, false, ARGS_GLOBAL><<<grid, block, 0, s>>>(g);
     }
 }
 

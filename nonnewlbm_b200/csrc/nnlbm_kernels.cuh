@@ -17,8 +17,8 @@
 // Work decomposition: a packed list of 32-cell row chunks of colliding cells (one warp
 // each, or one warp per two chunks in single-precision arithmetic), over all cases of
 // a launch group (same storage type and collision), followed by warps of 32 boundary
-// nodes.  Per-case parameters live in a device array indexed by the chunk's case (and in
-// parameter space for a single-case group).
+// nodes.  Per-case parameters live in a device array indexed by the chunk's case, and in
+// parameter space for groups of up to 16 cases (case_args).
 //
 // Open-plane nodes (TCPC IVC/SVC inflow and outlets, generic GEO_OUTFLOW_RIGHT_EQ) pull a
 // stencil re-centred one cell inward (sim_tcpc.cu:242-273, lbm_bc.h:147-152).  k_bc_gather
@@ -149,6 +149,21 @@ struct GroupArgs {
     // reads, so no launch needs a grid-wide count
     int* cursor;
 };
+
+// where a kernel finds the arguments of case ci: the device array, the parameters indexed
+// by the case, or, for a one-case group, the parameters' first entry at fixed offsets (read
+// as constant operands, with no indexed constant loads)
+enum : int { ARGS_GLOBAL = 0, ARGS_PARAM = 1, ARGS_ONE = 2 };
+template <int ARGS, class CT>
+__device__ __forceinline__ const CaseArgs<CT>& case_args(const GroupArgs<CT>& g, int ci)
+{
+    return ARGS == ARGS_ONE ? g.cp[0] : ARGS == ARGS_PARAM ? g.cp[ci] : g.cases[ci];
+}
+// the launch's choice for a group of n cases
+__host__ __device__ constexpr int args_mode(int n_cases)
+{
+    return n_cases == 1 ? ARGS_ONE : n_cases <= kParamCases ? ARGS_PARAM : ARGS_GLOBAL;
+}
 
 // programmatic dependent launch (sm_90+): the open-plane gather lets the step kernel of the
 // same step start at once; the step kernel waits for the gather's completion (and its
@@ -492,12 +507,12 @@ __device__ __forceinline__ void pair_load(const CaseArgs<float>& a, const Chunk&
 }
 
 // two plain chunks of one case (no finite-difference force) collide as a pair
-template <bool PARAM>
+template <int ARGS>
 __device__ __forceinline__ bool pairable(const GroupArgs<float>& g, const Chunk& ca, const Chunk& cb)
 {
     const int ci = ca.cflags & CH_CASE_MASK;
     return ((ca.cflags & cb.cflags) & CH_PLAIN) && ci == (cb.cflags & CH_CASE_MASK) &&
-           (PARAM ? g.cp[ci] : g.cases[ci]).cy_mode != CY_REF_FD;
+           case_args<ARGS>(g, ci).cy_mode != CY_REF_FD;
 }
 
 // 32 boundary nodes (open-plane nodes and GEO_INFLOW nodes, one per lane): each writes
@@ -537,7 +552,7 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
 // the step kernel: one warp per chunk of the work list (per two chunks where the variant
 // pairs them), then one warp per 32 boundary nodes.  Both write only the slots their own
 // cells read, so they run side by side.
-template <int DT, int COL, bool ODD, bool PARAM, bool PAIR>
+template <int DT, int COL, bool ODD, int ARGS, bool PAIR>
 __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::value))
     k_step(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
@@ -547,7 +562,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
     const int step = g.cursor[ODD ? 1 : 0];
     if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
     // the step's flags are the same for every case of the group
-    const int flags = (PARAM ? g.cp[0].ctl : g.cases[0].ctl)[step].flags;
+    const int flags = case_args<ARGS>(g, 0).ctl[step].flags;
     if constexpr (PAIR && pairs_chunks(DT, COL)) {
         // warp w takes chunks 2w and 2w + 1 (the host pads the list to an even length); a
         // pair that is not pairable (a face chunk, two cases, the finite-difference force)
@@ -556,8 +571,8 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
         if (w < np) {
             const Chunk ca = g.chunks[2 * w], cb = g.chunks[2 * w + 1];
             const int ci = ca.cflags & CH_CASE_MASK;
-            const CaseArgs<CT>& a = PARAM ? g.cp[ci] : g.cases[ci];
-            if (pairable<PARAM>(g, ca, cb)) {
+            const CaseArgs<CT>& a = case_args<ARGS>(g, ci);
+            if (pairable<ARGS>(g, ca, cb)) {
                 f2 f[27];
                 pair_load<DT, ODD>(a, ca, cb, lane, f);
                 pair_finish<DT, COL, ODD>(a, ca, cb, f, step, flags, lane);
@@ -565,7 +580,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
                 fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, step, flags, lane);
                 if (cb.fluid) {
                     const int cj = cb.cflags & CH_CASE_MASK;
-                    fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[cj] : g.cases[cj], g.cases + cj, cb, step, flags, lane);
+                    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, step, flags, lane);
                 }
             }
         } else {
@@ -575,7 +590,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
         if (w < g.n_chunks) {
             const Chunk ch = g.chunks[w];
             const int ci = ch.cflags & CH_CASE_MASK;
-            fluid_chunk<DT, COL, ODD>(PARAM ? g.cp[ci] : g.cases[ci], g.cases + ci, ch, step, flags, lane);
+            fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, ci), g.cases + ci, ch, step, flags, lane);
         } else {
             node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
         }
@@ -609,7 +624,7 @@ __device__ __forceinline__ void pull_triples(const CaseArgs<typename Storage<DT>
     for (int q = 0; q < 27; ++q) f[q] = canon<DT, ODD>(a, xs[1 - cxq(q)], ys[1 - cyq(q)], zs[1 - czq(q)], q);
 }
 
-template <int DT, bool ODD, bool PARAM>
+template <int DT, bool ODD, int ARGS>
 __global__ void __launch_bounds__(64) k_bc_gather(const __grid_constant__ GroupArgs<typename Storage<DT>::CT> g)
 {
     using CT = typename Storage<DT>::CT;
@@ -619,7 +634,7 @@ __global__ void __launch_bounds__(64) k_bc_gather(const __grid_constant__ GroupA
     // {cell, case, node index, label}: the stencil loads depend on nothing but this record
     // (and the case's arguments, from the parameters where the group is small)
     const int4 e = g.gather[t];
-    const CaseArgs<CT>& a = PARAM ? g.cp[e.y] : g.cases[e.y];
+    const CaseArgs<CT>& a = case_args<ARGS>(g, e.y);
     const StepCtl<CT>& ctl = a.ctl[g.cursor[ODD ? 1 : 0]];
     const int c = e.x, k = e.z;
     const int lab = e.w;
@@ -735,11 +750,11 @@ using StepLauncher = void (*)(bool odd, bool after_gather, bool paired, dim3 gri
                               const void* group_args);
 
 // launch of one step-kernel variant: one warp per chunk (per pair)
-template <int DT, int COL, bool ODD, bool PARAM, bool PAIR>
+template <int DT, int COL, bool ODD, int ARGS, bool PAIR>
 void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
     if (!after_gather) {
-        k_step<DT, COL, ODD, PARAM, PAIR><<<grid, block, 0, s>>>(g);
+        k_step<DT, COL, ODD, ARGS, PAIR><<<grid, block, 0, s>>>(g);
         return;
     }
     cudaLaunchConfig_t cfg = {};
@@ -752,19 +767,24 @@ void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t 
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_step<DT, COL, ODD, PARAM, PAIR>, g);
+    cudaLaunchKernelEx(&cfg, k_step<DT, COL, ODD, ARGS, PAIR>, g);
 }
 
 template <int DT, int COL, bool PAIR>
 void launch_step_form(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
-    // PARAM: the cases' arguments are in parameter space (g.cp)
-    if (g.n_cases <= kParamCases) {
-        if (odd) launch_step_variant<DT, COL, true, true, PAIR>(after_gather, grid, block, s, g);
-        else launch_step_variant<DT, COL, false, true, PAIR>(after_gather, grid, block, s, g);
-    } else {
-        if (odd) launch_step_variant<DT, COL, true, false, PAIR>(after_gather, grid, block, s, g);
-        else launch_step_variant<DT, COL, false, false, PAIR>(after_gather, grid, block, s, g);
+    switch (args_mode(g.n_cases)) {
+    case ARGS_ONE:
+        if (odd) launch_step_variant<DT, COL, true, ARGS_ONE, PAIR>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, ARGS_ONE, PAIR>(after_gather, grid, block, s, g);
+        break;
+    case ARGS_PARAM:
+        if (odd) launch_step_variant<DT, COL, true, ARGS_PARAM, PAIR>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, ARGS_PARAM, PAIR>(after_gather, grid, block, s, g);
+        break;
+    default:
+        if (odd) launch_step_variant<DT, COL, true, ARGS_GLOBAL, PAIR>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, ARGS_GLOBAL, PAIR>(after_gather, grid, block, s, g);
     }
 }
 
