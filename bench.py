@@ -433,7 +433,7 @@ def run_ours(a, dist: Dist) -> int:
     t_e2e = dist.max(t_e2e)
     e2e = fluid * a.e2e_steps * dist.world / t_e2e / 1e6
     h2d = 32 if w.dtype != "f64" else 56  # the step's control row
-    d2h = 88  # the context's status block: step cursors, watchdog flag, mass/flux sums
+    d2h = 16 + 32 * 64 + 8  # the context's status block: step cursors, 32 stripes of mass/flux sums, watchdog flag
     lat.close()
 
     if dist.rank == 0:

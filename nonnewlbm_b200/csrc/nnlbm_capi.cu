@@ -142,12 +142,14 @@ struct Group {
 
 // every word the host reads back after a step, in one device block (and one pinned host
 // mirror) so that a synchronous step costs one small copy: per launch group 4 ints (the
-// two step cursors), per case 8 doubles (the reductions) and 2 ints (the watchdog flag).
-// The cursors and the sums lead, so that one memset clears what a step call restarts.
+// two step cursors), per case kRedStripes x 8 doubles (the striped reductions) and 2 ints
+// (the watchdog flag).  The cursors and the sums lead, so that one memset clears what a
+// step call restarts.
+constexpr size_t kRedBytes = (size_t)kRedStripes * 8 * sizeof(double);
 struct StatusLayout {
     size_t cur, red, err, bytes;
     explicit StatusLayout(size_t n_slots)
-        : cur(0), red(16 * n_slots), err(80 * n_slots), bytes(88 * n_slots) {}
+        : cur(0), red(16 * n_slots), err(red + kRedBytes * n_slots), bytes(err + 8 * n_slots) {}
 };
 
 struct nnlbm_ctx {
@@ -442,7 +444,7 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = t
             CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
             c.ctl_dev = buf;
         }
-        if (reset && (flags & NNLBM_STEP_REDUCE)) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
+        if (reset && (flags & NNLBM_STEP_REDUCE)) CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
     }
     if ((rc = prepare_group(ctx, g)) != NNLBM_OK) return rc;
     if (reset) CK(cudaMemsetAsync(g.d_ints, 0, 2 * sizeof(int), ctx->stream));
@@ -672,7 +674,7 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
         }
         c.df = (char*)c.df_base + kDfPad;
         c.d_err = (int*)(ctx->d_status + sl.err) + 2 * i;
-        c.d_red = (double*)(ctx->d_status + sl.red) + 8 * i;
+        c.d_red = (double*)(ctx->d_status + sl.red + kRedBytes * i);
         c.label.assign((size_t)c.N, (uint8_t)L_WALL);
         c.dlabel = c.label;
         // launch groups: cases of one storage type and collision run in the same kernels
@@ -1065,7 +1067,12 @@ int nnlbm_reduce(nnlbm_ctx* ctx, int ic, double* out5)
     CK(cudaSetDevice(ctx->device));
     // a synchronous step has just read the sums back with its cursors and watchdog flags
     if (!ctx->status_fresh && (rc = read_status(ctx)) != NNLBM_OK) return rc;
-    memcpy(out5, (const double*)(ctx->h_status + StatusLayout(ctx->cases.size()).red) + 8 * ic, 5 * sizeof(double));
+    const double* r = (const double*)(ctx->h_status + StatusLayout(ctx->cases.size()).red + kRedBytes * ic);
+    for (int k = 0; k < 5; ++k) {
+        double v = 0.0;
+        for (int i = 0; i < kRedStripes; ++i) v += r[8 * i + k];
+        out5[k] = v;
+    }
     return NNLBM_OK;
 }
 
@@ -1277,7 +1284,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
             Case& c = ctx->cases[ic];
             rc = f64 ? upload_ctl_rows<double>(ctx, c, n_steps, flags) : upload_ctl_rows<float>(ctx, c, n_steps, flags);
             if (rc != NNLBM_OK) return rc;
-            if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, 5 * sizeof(double), ctx->stream));
+            if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
         }
         // the two cursors start at zero for every group; the group's steps, in stream
         // order, finish before the next group clears them again

@@ -105,7 +105,7 @@ struct CaseArgs {
     void* stats;               // [6][N] (double or float) or null
     int stats_f64, pad1;
     const StepCtl<CT>* ctl;
-    double* red;               // [5] mass, Q_ivc, Q_svc, Q_out5, Q_out6
+    double* red;               // [kRedStripes][8]: stripes of {mass, Q_ivc, Q_svc, Q_out5, Q_out6}
     int* err;                  // watchdog flag
     // per-slot base addresses of a plain chunk's accesses, each the population array of one
     // slot already offset by the cell shift of the access, so that an address is one
@@ -179,6 +179,13 @@ __device__ __forceinline__ typename Storage<DT>::T* qptr(const CaseArgs<typename
 }
 
 __device__ __forceinline__ int wrapc(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// the FP64 reductions of a case land in kRedStripes stripes of 8 doubles (64 bytes apart),
+// picked by warp or node index, so that thousands of warps do not serialise on one
+// address in L2; the host adds the stripes up when it reads the sums
+constexpr int kRedStripes = 32;
+__device__ __forceinline__ double* red_stripe(double* red, int i) { return red + 8 * (i & (kRedStripes - 1)); }
+__device__ __forceinline__ int global_warp() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
 
 __device__ __forceinline__ double warp_sum(double v)
 {
@@ -408,7 +415,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
     }
     if (flags & F_REDUCE) {
         const double s0 = warp_sum(mass);
-        if (lane == 0 && s0 != 0.0) atomicAdd(a.red, s0);
+        if (lane == 0 && s0 != 0.0) atomicAdd(red_stripe(a.red, global_warp()), s0);
     }
 }
 
@@ -483,7 +490,7 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Chun
     }
     if (flags & F_REDUCE) {
         const double s0 = warp_sum(mass);
-        if (lane == 0 && s0 != 0.0) atomicAdd(a.red, s0);
+        if (lane == 0 && s0 != 0.0) atomicAdd(red_stripe(a.red, global_warp()), s0);
     }
 }
 
@@ -545,7 +552,7 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
     const double qn = node_outputs<CT>(a, flags, lab, c, rho, ux, uy, uz);
     if ((flags & F_REDUCE) && qn != 0.0) {
         const int slot = lab == L_IN_L ? 1 : lab == L_IN_R ? 2 : lab == L_OUT_F ? 3 : lab == L_OUT_B ? 4 : 0;
-        if (slot) atomicAdd(a.red + slot, qn);
+        if (slot) atomicAdd(red_stripe(a.red, k) + slot, qn);
     }
 }
 
