@@ -206,6 +206,13 @@ int nnlbm_get_stats(nnlbm_ctx* ctx, int ic, double* out, int64_t* n_accumulated)
 int nnlbm_export_df(nnlbm_ctx* ctx, int ic, double* out);
 int nnlbm_import_df(nnlbm_ctx* ctx, int ic, const double* in);
 
+/* Restore state saved by a checkpoint: the mean/rms sums in the layout of nnlbm_get_stats
+ * with their step count, and every macro field ([NNLBM_M_N][nz][ny][nx], the order above;
+ * CY_REF_FD steps read the previous step's velocity from it).  Replaces the hmacro reload of
+ * State::loadState (state.hpp:1744-1756, saveAndLoadState :1552-1721). */
+int nnlbm_import_stats(nnlbm_ctx* ctx, int ic, const double* in, int64_t n_accumulated);
+int nnlbm_import_macro(nnlbm_ctx* ctx, int ic, const double* in);
+
 /* FP64 sums of the last step that had NNLBM_STEP_REDUCE: {mass of FLUID+PERIODIC cells,
  * Q_ivc, Q_svc, Q_outlet5, Q_outlet6}, lattice units, inflow positive at 3/4 and outflow
  * positive at 5/6 (postprocess/compute_flows.py:107-147).  Right after a synchronous

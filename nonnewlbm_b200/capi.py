@@ -23,11 +23,12 @@ CY_NONE, CY_REF_FD, CY_LOCAL_NEQ = 0, 1, 2
 CY_MODES = {"none": 0, "ref-fd": 1, "ref_fd": 1, "local-neq": 2, "local_neq": 2}
 STEP_STATS, STEP_MACRO, STEP_REDUCE, STEP_ASYNC = 1, 2, 4, 8
 M_RHO, M_VX, M_VY, M_VZ, M_FX, M_FY, M_FZ, M_S11, M_S12, M_S13, M_S22, M_S32, M_S33 = range(13)
+M_N = 13
 
 EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
     "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_step_noalloc", "nnlbm_stat_reset", "nnlbm_get_macro",
-    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_step_info", "nnlbm_profile_step",
+    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_import_stats", "nnlbm_import_macro", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_step_info", "nnlbm_profile_step",
     "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels", "nnlbm_sync",
 ]
 
@@ -77,6 +78,8 @@ def lib():
         L.nnlbm_get_stats.argtypes = [_vp, i, _dp, _i64p]
         L.nnlbm_export_df.argtypes = [_vp, i, _dp]
         L.nnlbm_import_df.argtypes = [_vp, i, _dp]
+        L.nnlbm_import_stats.argtypes = [_vp, i, _dp, ctypes.c_int64]
+        L.nnlbm_import_macro.argtypes = [_vp, i, _dp]
         L.nnlbm_reduce.argtypes = [_vp, i, _dp]
         L.nnlbm_autotune.argtypes = [_vp]
         L.nnlbm_autotune_flags.argtypes = [_vp, i]

@@ -778,6 +778,7 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
     c.self_prof.assign(self_cell.size() * 3, 0.0);
     c.n_fluid = nfl; c.left_area = la; c.right_area = ra; c.n_inflow_eq = neq; c.n_bc = nbc;
     CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream)); // no queued step still reads the old labels
     CK(cudaMemcpy(c.d_label, dl.data(), (size_t)c.N, cudaMemcpyHostToDevice));
     c.has_map = true;
     rebuild_case_args(ctx, c);
@@ -980,6 +981,8 @@ int nnlbm_get_macro(nnlbm_ctx* ctx, int ic, int field, double* out)
         if ((rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
         CK(cudaStreamSynchronize(ctx->stream));
     }
+    // the copies below run on the legacy stream: let the context's queued steps finish first
+    CK(cudaStreamSynchronize(ctx->stream));
     if (c.ct_bytes == 8) {
         CK(cudaMemcpy(out, (char*)c.d_macro + (size_t)field * c.N * 8, (size_t)c.N * 8, cudaMemcpyDeviceToHost));
     } else {
@@ -1000,12 +1003,56 @@ int nnlbm_get_stats(nnlbm_ctx* ctx, int ic, double* out, int64_t* n_accumulated)
     CK(cudaSetDevice(ctx->device));
     const size_t n = (size_t)6 * c.N;
     if (!c.d_stats) { memset(out, 0, n * sizeof(double)); return NNLBM_OK; }
+    CK(cudaStreamSynchronize(ctx->stream));
     if (c.d.stats_f64) {
         CK(cudaMemcpy(out, c.d_stats, n * 8, cudaMemcpyDeviceToHost));
     } else {
         std::vector<float> tmp(n);
         CK(cudaMemcpy(tmp.data(), c.d_stats, n * 4, cudaMemcpyDeviceToHost));
         for (size_t i = 0; i < n; ++i) out[i] = tmp[i];
+    }
+    return NNLBM_OK;
+}
+
+int nnlbm_import_stats(nnlbm_ctx* ctx, int ic, const double* in, int64_t n_accumulated)
+{
+    int rc = check_case(ctx, ic);
+    if (rc) return rc;
+    if (!in || n_accumulated < 0) return set_err(ctx, NNLBM_ERR_ARG, "null input or negative step count");
+    Case& c = ctx->cases[ic];
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = ensure_stats(ctx, c)) != NNLBM_OK) return rc;
+    const size_t n = (size_t)6 * c.N;
+    if (c.d.stats_f64) {
+        CK(cudaMemcpyAsync(c.d_stats, in, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+        std::vector<float> tmp(n);
+        for (size_t i = 0; i < n; ++i) tmp[i] = (float)in[i];
+        CK(cudaMemcpyAsync(c.d_stats, tmp.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    c.n_stats = n_accumulated;
+    return NNLBM_OK;
+}
+
+int nnlbm_import_macro(nnlbm_ctx* ctx, int ic, const double* in)
+{
+    int rc = check_case(ctx, ic);
+    if (rc) return rc;
+    if (!in) return set_err(ctx, NNLBM_ERR_ARG, "null input");
+    Case& c = ctx->cases[ic];
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
+    const size_t n = (size_t)M_N * c.N;
+    if (c.ct_bytes == 8) {
+        CK(cudaMemcpyAsync(c.d_macro, in, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+        std::vector<float> tmp(n);
+        for (size_t i = 0; i < n; ++i) tmp[i] = (float)in[i];
+        CK(cudaMemcpyAsync(c.d_macro, tmp.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
     }
     return NNLBM_OK;
 }
@@ -1019,6 +1066,7 @@ int nnlbm_export_df(nnlbm_ctx* ctx, int ic, double* out)
     CK(cudaSetDevice(ctx->device));
     const size_t eb = kStorageBytes[c.d.dtype];
     std::vector<char> raw(27 * c.q_stride * eb);
+    CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpy(raw.data(), c.df, raw.size(), cudaMemcpyDeviceToHost));
     const int nx = c.d.nx, ny = c.d.ny, nz = c.d.nz;
     for (int q = 0; q < 27; ++q)
@@ -1054,7 +1102,9 @@ int nnlbm_import_df(nnlbm_ctx* ctx, int ic, const double* in)
                     encode(c, raw.data() + (size_t)slot * c.q_stride * eb, i, q,
                            in[(size_t)q * c.N + x + (size_t)nx * (y + (size_t)ny * z)]);
                 }
-    CK(cudaMemcpy(c.df, raw.data(), raw.size(), cudaMemcpyHostToDevice));
+    // on the context's stream, after whatever steps it still holds
+    CK(cudaMemcpyAsync(c.df, raw.data(), raw.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     c.has_state = true;
     return NNLBM_OK;
 }

@@ -164,6 +164,22 @@ class Lattice:
             raise ValueError("population array size does not match the lattice")
         self._chk(capi.lib().nnlbm_import_df(self.h, ic, capi.dptr(a)))
 
+    def import_stats(self, sums: np.ndarray, n_accumulated: int, ic: int = 0) -> None:
+        a = np.ascontiguousarray(sums, dtype=np.float64).reshape(-1)
+        if a.size != 6 * self.ncells(ic):
+            raise ValueError("mean/rms array size does not match the lattice")
+        self._chk(capi.lib().nnlbm_import_stats(self.h, ic, capi.dptr(a), int(n_accumulated)))
+
+    def macro_all(self, ic: int = 0) -> np.ndarray:
+        """Every macro field, [M_N][nz][ny][nx]."""
+        return np.stack([self.macro(k, ic) for k in range(capi.M_N)])
+
+    def import_macro(self, fields: np.ndarray, ic: int = 0) -> None:
+        a = np.ascontiguousarray(fields, dtype=np.float64).reshape(-1)
+        if a.size != capi.M_N * self.ncells(ic):
+            raise ValueError("macro array size does not match the lattice")
+        self._chk(capi.lib().nnlbm_import_macro(self.h, ic, capi.dptr(a)))
+
     def reduce(self, ic: int = 0) -> np.ndarray:
         out = np.zeros(5)
         self._chk(capi.lib().nnlbm_reduce(self.h, ic, capi.dptr(out)))

@@ -12,7 +12,11 @@ boundary setup flags ``terminate``).  The step itself runs in libnnlbm.so.
 
 Extra options of this build: --dtype (f32 default, f16, bf16, f64), --collision (CUM
 default; KBC_N1..N4, KBC_C1..C4, MRT_LES, BGK), --cy-mode (none = the single-rank reference,
-ref-fd, local-neq), --equilibrium, --device, --results-root, --ramp-steps.
+ref-fd, local-neq), --equilibrium, --device, --results-root, --ramp-steps, and the state
+checkpoint knobs the reference keeps in State (state.h:229-257): --wall-time SECONDS (save
+the state and stop when reached) and --savestate-period SECONDS (wall-clock period of the
+`savestate` flag check).  A `results_<id>/loadstate` flag resumes from the saved state
+(checkpoint.py).
 """
 from __future__ import annotations
 
@@ -25,7 +29,7 @@ from pathlib import Path
 
 import numpy as np
 
-from . import capi, units, vtk
+from . import capi, checkpoint, units, vtk
 from .lattice import CaseSpec, Lattice
 
 USAGE = ("Usage: ./sim_tcpc --geometry geometry.vtk --material newtonian|sx|gx "
@@ -60,6 +64,8 @@ class TcpcOptions:
     device: int = 0
     results_root: str = "."
     ramp_steps: int = 0
+    wall_time: float = -1.0         # State::wallTime (state.h:256), seconds; <= 0 disables
+    savestate_period: float = -1.0  # cnt[SAVESTATE].period in wall-clock seconds (core.h:1594)
 
 
 def parse_args(argv) -> TcpcOptions:
@@ -67,7 +73,7 @@ def parse_args(argv) -> TcpcOptions:
     o = TcpcOptions()
     num = {"--ivc-mls": "ivc_mls", "--svc-mls": "svc_mls", "--final-time": "final_time", "--vtk-period": "vtk_period",
            "--print-period": "print_period", "--stat-reset-period": "stat_reset_period",
-           "--lbm-viscosity": "lbm_viscosity"}
+           "--lbm-viscosity": "lbm_viscosity", "--wall-time": "wall_time", "--savestate-period": "savestate_period"}
     text = {"--geometry": "geometry", "--material": "material", "--case-id": "case_id", "--output-id": "case_id",
             "--dtype": "dtype", "--collision": "collision", "--cy-mode": "cy_mode", "--equilibrium": "equilibrium",
             "--results-root": "results_root"}
@@ -211,12 +217,46 @@ class TcpcRun:
         return p
 
     # -- the time loop (core.h:1473-1628) ------------------------------------------------
+    # -- checkpoint (state.hpp:1724-1756, core.h:1511-1602) --------------------------------
+    _CNT_INDEX = {"stat": checkpoint.STAT_RESET, "print": checkpoint.PRINT, "vtk": checkpoint.VTK3D,
+                  "save": checkpoint.SAVESTATE}
+
+    def save_state(self, cnt, forced: bool = False) -> bool:
+        """State::saveState: with the `savestate` flag present (or forced) write the state;
+        the flag is then replaced by `savestate_done`, and a forced save creates `loadstate`."""
+        if not (forced or checkpoint.flag_exists(self.dir, "savestate")):
+            return False
+        self.log("[saveState invoked]")
+        counters = {self._CNT_INDEX[k]: (c.count, c.period) for k, c in cnt.items()}
+        checkpoint.save_state(self.dir, self.lat, self.iterations, self.o.final_time, counters, self.map)
+        if not forced:
+            checkpoint.flag_delete(self.dir, "savestate")
+            checkpoint.flag_create(self.dir, "savestate_done")
+        else:
+            checkpoint.flag_create(self.dir, "loadstate")
+        return True
+
+    def load_state(self, cnt) -> None:
+        """State::loadState: the saved populations, fields, sums, iteration and counters."""
+        self.log("[loadState invoked]")
+        cfg = checkpoint.load_state(self.dir, self.lat, labels=self.map)
+        self.iterations = cfg["iterations"]
+        self.prev_iter = self.iterations - cfg["stats_count"]
+        for k, c in cnt.items():
+            if self._CNT_INDEX[k] in cfg["counters"]:
+                c.count = cfg["counters"][self._CNT_INDEX[k]][0]
+
     def run(self) -> int:
         o = self.o
-        cnt = {"print": Counter(o.print_period), "stat": Counter(o.stat_reset_period), "vtk": Counter(o.vtk_period)}
+        cnt = {"print": Counter(o.print_period), "stat": Counter(o.stat_reset_period), "vtk": Counter(o.vtk_period),
+               "save": Counter(o.savestate_period)}
+        if checkpoint.flag_exists(self.dir, "loadstate"):
+            self.load_state(cnt)
         self.log(f"\nSTART: simulation LBM:{o.collision} dimensions {self.shape[0]} x {self.shape[1]} x {self.shape[2]} "
                  f"lbmVisc {self.conv['nu']:e} physDl {self.dx:e} physDt {self.dt:e}")
         t_wall0 = time.perf_counter()
+        # the wall clock is checked after every call; with a checkpoint knob on, calls stay short
+        max_chunk = 100 if (o.wall_time > 0 or o.savestate_period > 0) else 100000
         t1 = time.perf_counter()
         prev_mlups_it = 0
         total = int(np.prod(self.shape))
@@ -230,7 +270,7 @@ class TcpcRun:
                 k += 1
                 t = self.dt * (self.iterations + k)
                 if (cnt["vtk"].action(t) or cnt["stat"].action(t) or cnt["print"].action(t) or t > o.final_time
-                        or self.terminate or k >= 100000):
+                        or self.terminate or k >= max_chunk):
                     break
             if o.ramp_steps > 0:
                 rows = []
@@ -250,6 +290,15 @@ class TcpcRun:
                 eta = wt * (o.final_time - self.phys_time()) / max(self.phys_time(), 1e-30)
                 self.log(f"MLUPS={lups * 1e-6:.1f} iter={self.iterations} t={self.phys_time():1.3f}s dt={self.dt:1.2e} "
                          f"lbmVisc={self.conv['nu']:1.2e} WT={wt:.0f}s ETA={eta:.0f}s")
+            wall = time.perf_counter() - t_wall0
+            if o.wall_time > 0 and wall >= o.wall_time:
+                self.log(f"wallTime reached: {wall:.0f} / {o.wall_time:.0f} [sec]")
+                self.log("maximum wall time reached")
+                self.save_state(cnt, forced=True)
+                quit_ = True
+            elif cnt["save"].action(wall):
+                self.save_state(cnt)
+                cnt["save"].count += 1
             if self.phys_time() > o.final_time:
                 self.log("physFinalTime reached")
                 quit_ = True
