@@ -63,3 +63,29 @@ def test_resume_matches_uninterrupted(tmp_path, dtype, cy_mode):
         # FP32 storage: the canonical FP64 file rounds each population once on reload
         assert max_rel(a, b, dead) <= 1e-5
         assert np.max(np.abs(sa - sb)) <= 1e-5 * max(1.0, np.max(np.abs(sb)))
+
+
+def test_driver_wall_time_then_resume(tmp_path):
+    """sim_tcpc's loop (core.h:1578-1602) through the driver: the wall time is reached after the
+    first call, the state is saved and `loadstate` left behind; the next start resumes from
+    that iteration and runs to the final time."""
+    from nonnewlbm_b200 import tcpc, units, vtk
+
+    dx = 2.5e-4
+    wall = small_junction()
+    geo = tmp_path / "geometry.vtk"
+    vtk.write_geometry(geo, wall, dx)
+    dt = units.lattice_units(units.material_by_name("newtonian"), dx, 1e-4)["dt"]
+    final = 250.5 * dt
+    base = ["--geometry", str(geo), "--material", "newtonian", "--ivc-mls", "0.02", "--svc-mls", "0.012",
+            "--case-id", "ck", "--final-time", repr(final), "--vtk-period", "1e9", "--print-period", "1e9",
+            "--results-root", str(tmp_path)]
+    results = tmp_path / "results_ck"
+    assert tcpc.main(base + ["--wall-time", "1e-9"]) == 0
+    assert C.flag_exists(results, "loadstate")
+    saved = C.read_config(results)["iterations"]
+    assert 0 < saved <= 100
+    assert tcpc.main(base) == 0
+    log = (results / "log_rank000").read_text()
+    assert "maximum wall time reached" in log and "[loadState invoked]" in log
+    assert log.rstrip().endswith("physFinalTime reached")
