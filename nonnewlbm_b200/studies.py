@@ -98,15 +98,18 @@ def _setup(lat: Lattice, cases: list[StudyCase], first: int = 0) -> list[dict]:
     return areas
 
 
-def run_batch(cases: list[StudyCase], steps: int = 200, warmup: int = 20, device: int = 0) -> dict:
+def run_batch(cases: list[StudyCase], steps: int = 200, warmup: int = 20, device: int = 0, autotune: bool = True) -> dict:
     """Batched (one context, one launch group) against sequential (one context per case,
     stepped one after another) wall time of ``steps`` steps of every case, each measured
     after ``warmup`` steps; the per-step inflow rows (with the pulsation) are uploaded in
-    one call before each timed run, outside the clock."""
+    one call before each timed run, outside the clock.  With ``autotune`` both the batched
+    context and every single one pick their launch shape first (nnlbm_autotune)."""
     fluid = 0
     # batched
     lat = Lattice([c.spec for c in cases], device=device)
     areas = _setup(lat, cases)
+    if autotune:
+        lat.autotune()
     lat.step(warmup)
     for k, c in enumerate(cases):
         lat.set_schedule(_schedule(c, areas[k], warmup, steps), ic=k)
@@ -120,6 +123,8 @@ def run_batch(cases: list[StudyCase], steps: int = 200, warmup: int = 20, device
     for c in cases:
         one = Lattice(c.spec, device=device)
         a = _setup(one, [c])[0]
+        if autotune:
+            one.autotune()
         one.step(warmup)
         one.set_schedule(_schedule(c, a, warmup, steps))
         t0 = time.perf_counter()
@@ -127,6 +132,7 @@ def run_batch(cases: list[StudyCase], steps: int = 200, warmup: int = 20, device
         t_seq += time.perf_counter() - t0
         one.close()
     return {"cases": len(cases), "steps": steps, "fluid_cells": int(fluid), "dtype": cases[0].spec.dtype,
+            "autotuned": bool(autotune),
             "batched_s": t_batched, "sequential_s": t_seq, "gain": t_seq / t_batched,
             "batched_mlups": fluid * steps / t_batched / 1e6, "sequential_mlups": fluid * steps / t_seq / 1e6,
             "scales": [round(c.scale, 4) for c in cases]}
