@@ -232,6 +232,11 @@ int nnlbm_autotune(nnlbm_ctx* ctx);
  * fields are restored afterwards like the populations. */
 int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags);
 
+/* Set the step kernel's launch shape by hand for every launch group: `block` threads (64,
+ * 128 or 256) and 1 or 2 cells a thread (2 applies to the single-precision cumulant, BGK
+ * and MRT; the others step one).  Replaces --block-size (sim_tcpc.cu:118-119). */
+int nnlbm_set_launch(nnlbm_ctx* ctx, int block, int cells_per_thread);
+
 /* Number of populations-kernel launches and bytes moved per step for case ic
  * (roofline bookkeeping). */
 int nnlbm_step_info(nnlbm_ctx* ctx, int ic, int64_t* fluid_cells, int64_t* bc_cells,

@@ -28,7 +28,7 @@ M_N = 13
 EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
     "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_step_noalloc", "nnlbm_stat_reset", "nnlbm_get_macro",
-    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_import_stats", "nnlbm_import_macro", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_step_info", "nnlbm_profile_step",
+    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_import_stats", "nnlbm_import_macro", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_set_launch", "nnlbm_step_info", "nnlbm_profile_step",
     "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels", "nnlbm_sync",
 ]
 
@@ -83,6 +83,7 @@ def lib():
         L.nnlbm_reduce.argtypes = [_vp, i, _dp]
         L.nnlbm_autotune.argtypes = [_vp]
         L.nnlbm_autotune_flags.argtypes = [_vp, i]
+        L.nnlbm_set_launch.argtypes = [_vp, i, i]
         L.nnlbm_step_info.argtypes = [_vp, i, _i64p, _i64p, _i64p, _dp]
         L.nnlbm_profile_step.argtypes = [_vp, i, ctypes.c_int64, i, _dp, _i64p]
         L.nnlbm_sync.argtypes = [_vp]

@@ -1214,6 +1214,21 @@ int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags)
 
 int nnlbm_autotune(nnlbm_ctx* ctx) { return nnlbm_autotune_flags(ctx, 0); }
 
+int nnlbm_set_launch(nnlbm_ctx* ctx, int block, int cells_per_thread)
+{
+    if (!ctx) return NNLBM_ERR_ARG;
+    if (block != 64 && block != 128 && block != 256)
+        return set_err(ctx, NNLBM_ERR_ARG, "block size %d: use 64, 128 or 256", block);
+    if (cells_per_thread != 1 && cells_per_thread != 2)
+        return set_err(ctx, NNLBM_ERR_ARG, "cells per thread %d: use 1 or 2", cells_per_thread);
+    for (Group& g : ctx->groups) {
+        g.block = block;
+        g.paired = cells_per_thread == 2 && pairs_chunks(g.dtype, g.collision);
+        g.gen++; // the graphs captured another launch shape
+    }
+    return NNLBM_OK;
+}
+
 int nnlbm_step_info(nnlbm_ctx* ctx, int ic, int64_t* fluid_cells, int64_t* bc_cells, int64_t* launches_per_step,
                     double* bytes_per_step)
 {

@@ -137,6 +137,10 @@ class Lattice:
         flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0)
         self._chk(capi.lib().nnlbm_autotune_flags(self.h, flags))
 
+    def set_launch(self, block: int = 256, cells_per_thread: int = 2) -> None:
+        """Fix the step kernel's launch shape instead of autotuning it."""
+        self._chk(capi.lib().nnlbm_set_launch(self.h, int(block), int(cells_per_thread)))
+
     def stat_reset(self, ic: int | None = None) -> None:
         for k in self._cases(ic):
             self._chk(capi.lib().nnlbm_stat_reset(self.h, k))

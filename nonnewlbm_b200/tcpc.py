@@ -252,6 +252,9 @@ class TcpcRun:
                "save": Counter(o.savestate_period)}
         if checkpoint.flag_exists(self.dir, "loadstate"):
             self.load_state(cnt)
+        # the launch shape of the step kernel is timed on copies of the state, not taken from
+        # --block-size (sim_tcpc.cu:118-119)
+        self.lat.autotune(stats=True, macro=True)
         self.log(f"\nSTART: simulation LBM:{o.collision} dimensions {self.shape[0]} x {self.shape[1]} x {self.shape[2]} "
                  f"lbmVisc {self.conv['nu']:e} physDl {self.dx:e} physDt {self.dt:e}")
         t_wall0 = time.perf_counter()

@@ -183,6 +183,30 @@ def test_fp32_collisions_vs_fp64_oracle(collision):
         assert err <= 2e-5, (O.COLLISIONS[collision], err)
 
 
+@pytest.mark.parametrize("cells", [1, 2])
+@pytest.mark.parametrize("collision,dtype,tol_u", [(0, "f32", 2e-5), (9, "f32", 2e-5), (10, "f32", 2e-5), (0, "f16", 2e-3)],
+                         ids=["CUM-f32", "MRT_LES-f32", "BGK-f32", "CUM-f16"])
+def test_both_launch_forms_vs_fp64_oracle(collision, dtype, tol_u, cells):
+    """The one-cell (64 registers) and the paired (two cells a thread) form of a collision that
+    pairs, each against the FP64 oracle after 200 steps, relative to the peak velocity."""
+    orc, lat = _tcpc_pair(collision, dtype=dtype)
+    lat.set_launch(128, cells)
+    orc.step(200)
+    lat.step(200, macro=True)
+    fluid = orc.get_map() == G.MAP_FLUID
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
+    for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
+        assert err <= tol_u, (O.COLLISIONS[collision], dtype, cells, err)
+
+
+def test_set_launch_rejects_bad_shapes():
+    orc, lat = _tcpc_pair(0, dtype="f32")
+    for block, cells in ((96, 1), (256, 3)):
+        with pytest.raises(capi.NnlbmError):
+            lat.set_launch(block, cells)
+
+
 @pytest.mark.parametrize("dtype,tol_u", [("f32", 5e-5), ("f16", 2e-3)])
 def test_reduced_precision_cy_local_neq(dtype, tol_u):
     """The cumulant with the local Carreau-Yasuda viscosity (solved two cells at a time in
