@@ -753,8 +753,6 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 x0 = std::max(x0 / align * align, end);
                 Chunk ch{};
                 ch.c0 = (int)id(x0, y, z);
-                ch.split = kChunk; // one row segment
-                ch.c1 = 0;
                 ch.yz = y | (z << 16);
                 for (int x = x0; x < std::min(nx, x0 + kChunk); ++x) {
                     const size_t i = id(x, y, z);
@@ -772,34 +770,9 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 ch.cflags = CH_FLUID | (face ? CH_FACE : 0) | (plain ? CH_PLAIN : 0);
                 chunks.push_back(ch);
             }
-    // a chunk's colliding cells span its first `span` lanes; two consecutive plain
-    // one-segment chunks whose spans fit in 32 lanes share a warp (short vessel rows would
-    // otherwise leave lanes idle): the second row's cells go to lanes span_a .. 31
-    auto span = [](unsigned m) { return m ? 32 - __builtin_clz(m) : 0; };
-    std::vector<Chunk> packed;
-    packed.reserve(chunks.size());
-    for (size_t k = 0; k < chunks.size(); ++k) {
-        const Chunk& a = chunks[k];
-        const bool mergeable = (a.cflags & CH_PLAIN) && a.split == kChunk;
-        if (mergeable && k + 1 < chunks.size()) {
-            const Chunk& b = chunks[k + 1];
-            const int sa = span(a.fluid), sb = span(b.fluid);
-            if ((b.cflags & CH_PLAIN) && b.split == kChunk && sa + sb <= kChunk) {
-                Chunk m = a;
-                m.split = sa;
-                m.c1 = b.c0 - sa;
-                m.fluid = a.fluid | (b.fluid << sa);
-                m.periodic = a.periodic | (b.periodic << sa);
-                packed.push_back(m);
-                ++k;
-                continue;
-            }
-        }
-        packed.push_back(a);
-    }
     c.label.assign(map, map + c.N);
     c.dlabel = dl;
-    c.chunks = packed;
+    c.chunks = chunks;
     c.self_cell = self_cell;
     c.gather_self = gather_self;
     c.self_prof.assign(self_cell.size() * 3, 0.0);

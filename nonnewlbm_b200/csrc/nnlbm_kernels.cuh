@@ -120,16 +120,9 @@ struct CaseArgs {
 // one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
 // and per lane (bit = lane) which cells collide and which of those are PERIODIC
 struct alignas(16) Chunk {
-    int c0, yz, cflags, split;
-    unsigned fluid, periodic;
-    int c1, pad0;
+    int c0, yz, cflags, pad0;
+    unsigned fluid, periodic, pad1, pad2;
 };
-// the cell of a lane: lanes below `split` take c0 + lane; a plain chunk that packs the
-// colliding spans of two short rows (split < 32) gives the rest c1 + lane
-__host__ __device__ __forceinline__ int chunk_cell(const Chunk& ch, int lane)
-{
-    return lane < ch.split ? ch.c0 + lane : ch.c1 + lane;
-}
 // chunk flags (bits 16.. of cflags, the case index below).  CH_PLAIN: no neighbour of any
 // colliding lane wraps around the box (the chunk is off the y/z faces and has no
 // colliding cell at x = 0 or nx-1)
@@ -357,7 +350,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
     double mass = 0.0;
     const unsigned bit = 1u << lane;
     if (ch.fluid & bit) {
-        const int c = chunk_cell(ch, lane);
+        const int c = ch.c0 + lane;
         const int64_t qs = a.qstride, sy = a.nx, sz = (int64_t)a.nx * a.ny;
         const bool plain = (ch.cflags & CH_PLAIN) != 0;
         // the wrapped neighbour cell x + sign c_q of a face chunk
@@ -459,7 +452,7 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Chun
     const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
     double mass = 0.0;
     if (fa || fb) {
-        const int cA = chunk_cell(ca, lane), cB = chunk_cell(cb, lane);
+        const int cA = ca.c0 + lane, cB = cb.c0 + lane;
         const f2 fx(a.fx), fy(a.fy), fz(a.fz);
         f2 rho, ux, uy, uz;
         density_velocity<f2>(f, fx, fy, fz, rho, ux, uy, uz);
@@ -509,7 +502,7 @@ __device__ __forceinline__ void pair_load(const CaseArgs<float>& a, const Chunk&
     using T = typename Storage<DT>::T;
     const unsigned bit = 1u << lane;
     const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
-    const int cA = chunk_cell(ca, lane), cB = chunk_cell(cb, lane);
+    const int cA = ca.c0 + lane, cB = cb.c0 + lane;
     const f2 isc(a.inv_scale);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
@@ -703,10 +696,10 @@ __global__ void __launch_bounds__(256) k_refd_velocity(const __grid_constant__ G
     const Chunk& ch = g.chunks[warp];
     const CaseArgs<CT>& a = g.cases[ch.cflags & CH_CASE_MASK];
     if (a.cy_mode != CY_REF_FD) return;
-    if (!(ch.fluid & (1u << lane))) return;
-    const int c = chunk_cell(ch, lane);
-    if ((a.label[c] & L_MASK) != L_FLUID) return;
-    const int x = c % a.nx, y = (c / a.nx) % a.ny, z = c / (a.nx * a.ny);
+    const int y = ch.yz & 0xffff, z = ch.yz >> 16;
+    const int x = ch.c0 - y * a.nx - z * a.nx * a.ny + lane;
+    const int c = ch.c0 + lane;
+    if (x >= a.nx || (a.label[c] & L_MASK) != L_FLUID) return;
     const int xs[3] = {x - 1, x, x + 1}, ys[3] = {y - 1, y, y + 1}, zs[3] = {z - 1, z, z + 1};
     CT f[27];
     pull_triples<DT, ODD>(a, xs, ys, zs, f);
@@ -727,9 +720,10 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
     const CaseArgs<CT>& a = g.cases[ch.cflags & CH_CASE_MASK];
     if (a.cy_mode != CY_REF_FD) return;
     const int sy = a.nx, sz = a.nx * a.ny;
-    if (!(ch.fluid & (1u << lane))) return;
-    const int c = chunk_cell(ch, lane);
-    if ((a.label[c] & L_MASK) != L_FLUID) return;
+    const int y = ch.yz & 0xffff, z = ch.yz >> 16;
+    const int x = ch.c0 - y * sy - z * sz + lane;
+    const int c = ch.c0 + lane;
+    if (x >= a.nx || (a.label[c] & L_MASK) != L_FLUID) return;
     CT* M = a.macro;
     const int64_t N = a.N;
     const int cn[6] = {c - 1, c + 1, c - sy, c + sy, c - sz, c + sz};
