@@ -70,13 +70,14 @@ template <> struct Storage<2> {
     using T = __half; using CT = float;
     __device__ static __forceinline__ CT from(T v, int q, CT isc) { return weight<float>(q) + __half2float(v) * isc; }
     __device__ static __forceinline__ CT load(const T* p, int64_t i, int q, CT isc) { return from(p[i], q, isc); }
-    __device__ static __forceinline__ void store(T* p, int64_t i, int q, CT v, CT sc) { p[i] = __float2half_rn((v - weight<float>(q)) * sc); }
+    // (v - w) sc as one fused v sc - w sc (four distinct w sc per thread)
+    __device__ static __forceinline__ void store(T* p, int64_t i, int q, CT v, CT sc) { p[i] = __float2half_rn(fmaf(v, sc, -(weight<float>(q) * sc))); }
 };
 template <> struct Storage<3> {
     using T = __nv_bfloat16; using CT = float;
     __device__ static __forceinline__ CT from(T v, int q, CT isc) { return weight<float>(q) + __bfloat162float(v) * isc; }
     __device__ static __forceinline__ CT load(const T* p, int64_t i, int q, CT isc) { return from(p[i], q, isc); }
-    __device__ static __forceinline__ void store(T* p, int64_t i, int q, CT v, CT sc) { p[i] = __float2bfloat16_rn((v - weight<float>(q)) * sc); }
+    __device__ static __forceinline__ void store(T* p, int64_t i, int q, CT v, CT sc) { p[i] = __float2bfloat16_rn(fmaf(v, sc, -(weight<float>(q) * sc))); }
 };
 
 // per-step control row written by the host before each nnlbm_step call and indexed by a
@@ -466,7 +467,7 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Chun
         for (int q = 0; q < 27; ++q) {
             T* p = (T*)(ODD ? a.slot_odd_st[q] : a.slot_even[oppq(q)]);
             const f2 w(weight<float>(q));
-            const f2 v = DT == 1 ? f[q] - w : (f[q] - w) * sc;
+            const f2 v = DT == 1 ? f[q] - w : mad(f[q], sc, -(w * sc));
             if (fa) p[cA] = Cook<DT>::put(v.v.x);
             if (fb) p[cB] = Cook<DT>::put(v.v.y);
         }
