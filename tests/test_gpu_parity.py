@@ -318,6 +318,23 @@ def test_batched_mixed_groups_and_sizes():
         assert np.array_equal(lat.stats(k)[0], singles[k].stats()[0])
 
 
+def test_reduce_sums_after_sync_async_and_plain_steps():
+    """The FP64 sums (striped over 32 addresses, added on the host) come back the same after a
+    synchronous step, after an asynchronous step and nnlbm_sync, and stay those of the last
+    reducing step across steps that do not reduce."""
+    lats = [_tcpc_pair(0)[1] for _ in range(2)]
+    lats[0].step(6, reduce=True)
+    r_sync = lats[0].reduce()
+    lats[1].step(6, reduce=True, wait=False)
+    lats[1].sync()
+    r_async = lats[1].reduce()
+    # FP64 atomic sums: the order of the additions may differ between runs
+    assert np.all(np.abs(r_sync - r_async) <= 1e-12 * np.maximum(1.0, np.abs(r_sync)))
+    lats[0].step(3)
+    assert np.array_equal(lats[0].reduce(), r_sync)
+    assert r_sync[0] > 0 and np.all(np.isfinite(r_sync))
+
+
 def test_async_steps_and_control_rows_match_sync():
     """Steps enqueued without waiting (NNLBM_STEP_ASYNC, then nnlbm_sync) and one-step calls
     whose unchanged control rows are not sent again give the same lattice as synchronous
