@@ -35,7 +35,8 @@ typedef enum {
     NNLBM_ERR_ARG = -1,     /* invalid argument, label, size or state */
     NNLBM_ERR_CUDA = -2,    /* a CUDA runtime call failed */
     NNLBM_ERR_NAN = -3,     /* the device watchdog saw a non-finite or out-of-range density */
-    NNLBM_ERR_TIMEOUT = -4, /* a bounded device wait gave up */
+    NNLBM_ERR_TIMEOUT = -4, /* reserved for a bounded device wait that gives up; no kernel of
+                               this library waits on another, so no call returns it today */
     NNLBM_ERR_OOM = -5,     /* device allocation failed */
     NNLBM_ERR_AREA = -6     /* zero inlet or outlet area after the TCPC boundary setup */
 } nnlbm_status;
@@ -155,11 +156,11 @@ int nnlbm_set_schedule(nnlbm_ctx* ctx, int ic, const double* rows, int64_t n);
  * applied to every step; NNLBM_STEP_MACRO and NNLBM_STEP_REDUCE apply to the last step. */
 int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags);
 
-/* Size of the one scratch array that nnlbm_step_noalloc uses on each device: two step
- * cursors (256 bytes) plus, per launch group, four values (rho, ux, uy, uz) of the
- * arithmetic type for each open-plane node that its own thread writes (nnlbm_step_info's
- * bc_cells bounds that count).  4 MiB holds 262,128 such nodes in FP32 arithmetic and
- * 131,064 in FP64. */
+/* Size of the one scratch array that nnlbm_step_noalloc uses on each device: the step
+ * cursors of up to 64 launch groups (1 KiB) plus, per launch group, four values (rho, ux, uy,
+ * uz) of the arithmetic type for each open-plane node that its own thread writes
+ * (nnlbm_step_info's bc_cells bounds that count).  4 MiB holds 262,080 such nodes in FP32
+ * arithmetic and 131,040 in FP64. */
 #define NNLBM_NOALLOC_SCRATCH_BYTES (4u << 20)
 
 /* nnlbm_step that allocates no device memory.  No counterpart in the reference (its
@@ -171,14 +172,17 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags);
  * must not meet an out-of-memory error in the middle of a run.
  *
  * Same kernels, arguments and results as nnlbm_step, run as plain launches (no CUDA
- * graph).  The per-call scratch of nnlbm_step (the two step cursors and the
- * gathered open-plane node values) lives instead in one file-scope device array of
- * NNLBM_NOALLOC_SCRATCH_BYTES per device.  Its address is looked up the first time this
- * function runs on a device (cudaGetSymbolAddress, with the device current), so that
- * first call should come before any stream capture.  Every call shares the array: the
- * cursors are cleared at the start of each group's steps (the node values are written
- * before they are read in every step and need no clearing), and calls that overlap in
- * time, from two contexts on one device or from two host threads, race on it.
+ * graph).  The per-call scratch of nnlbm_step (the step cursors and the gathered
+ * open-plane node values) lives instead in one file-scope device array of
+ * NNLBM_NOALLOC_SCRATCH_BYTES per device, which the library holds until the process exits.
+ * nnlbm_create looks its address up (cudaGetSymbolAddress, with the device current) and loads
+ * the code of every kernel the context can launch, so that neither happens, with the device
+ * memory it takes, inside this call under CUDA's lazy module loading.  Every call shares the
+ * array: the cursors are cleared at the start of each call (the node values are written
+ * before they are read in every step and need no clearing), and calls that overlap in time,
+ * from two contexts on one device or from two host threads, race on it.  With
+ * NNLBM_STEP_ASYNC the call returns once the steps are enqueued and nnlbm_sync checks them,
+ * as for nnlbm_step; the control rows are still copied from the host before it returns.
  *
  * It returns NNLBM_ERR_ARG, with a message, and launches nothing when a buffer would
  * have to be allocated first: a launch group whose work lists are not on the device yet

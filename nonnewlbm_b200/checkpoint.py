@@ -22,6 +22,8 @@ unconditionally and creates ``loadstate``.
 """
 from __future__ import annotations
 
+import os
+import shutil
 import time
 from pathlib import Path
 
@@ -57,31 +59,65 @@ def flag_exists(results: Path, flag: str) -> bool:
 
 
 # -- the state files (state.hpp:1552-1721) ----------------------------------------------------
+def _write(path: Path, data) -> None:
+    """One state file, flushed to the disk before it is closed."""
+    with open(path, "wb") as f:
+        if isinstance(data, np.ndarray):
+            data.tofile(f)
+        else:
+            f.write(data.encode())
+        f.flush()
+        os.fsync(f.fileno())
+
+
 def save_state(results: Path, lat, iterations: int, final_time: float, counters: dict, labels: np.ndarray,
                ic: int = 0) -> Path:
     """Write the state of case ic of `lat` (a Lattice) into results/current_state/.
-    `counters` maps counter index -> (count, period); missing counters are saved as (0, -1)."""
-    d = Path(results) / STATE_DIR
-    d.mkdir(parents=True, exist_ok=True)
+    `counters` maps counter index -> (count, period); missing counters are saved as (0, -1).
+
+    The files go to a sibling directory first and replace current_state/ only once all of
+    them are on the disk (the reference stages a save through a .tmp copy for the same
+    reason, state.hpp:1558-1572), so a job killed in the middle of a save leaves the previous
+    complete state behind; a caller creates the loadstate flag after this returns."""
+    results = Path(results)
+    d = results / STATE_DIR
+    tmp = results / (STATE_DIR + ".tmp")
+    old = results / (STATE_DIR + ".old")
+    for p in (tmp, old):
+        if p.exists():
+            shutil.rmtree(p)
+    tmp.mkdir(parents=True)
     nz, ny, nx = lat.shape(ic)
-    with open(_name(d, "config"), "w") as f:
-        f.write("".join(f"{v:d}\n" for v in (int(iterations), nx, ny, nz, nx, ny, nz)) + f"{float(final_time):e}\n")
+    _write(_name(tmp, "config"),
+           "".join(f"{v:d}\n" for v in (int(iterations), nx, ny, nz, nx, ny, nz)) + f"{float(final_time):e}\n")
     for c in range(MAX_COUNTER):
         count, period = counters.get(c, (0, -1.0))
-        with open(_name(d, f"cnt_{c}"), "w") as f:
-            f.write(f"{int(count):d}\n{float(period):e}\n")
-    lat.export_df(ic).astype(np.float64).tofile(_name(d, "df_0"))
-    np.ascontiguousarray(labels, dtype=np.uint8).tofile(_name(d, "map"))
-    lat.macro_all(ic).astype(np.float64).tofile(_name(d, "macro"))
+        _write(_name(tmp, f"cnt_{c}"), f"{int(count):d}\n{float(period):e}\n")
+    _write(_name(tmp, "df_0"), lat.export_df(ic).astype(np.float64))
+    _write(_name(tmp, "map"), np.ascontiguousarray(labels, dtype=np.uint8))
+    _write(_name(tmp, "macro"), lat.macro_all(ic).astype(np.float64))
     sums, n = lat.stats(ic)
-    sums.astype(np.float64).tofile(_name(d, "stats"))
-    with open(_name(d, "stats_count"), "w") as f:
-        f.write(f"{int(n):d}\n")
+    _write(_name(tmp, "stats"), sums.astype(np.float64))
+    _write(_name(tmp, "stats_count"), f"{int(n):d}\n")
+    # swap: the previous state steps aside, the new one takes its name, the old one goes
+    if d.exists():
+        os.rename(d, old)
+    os.rename(tmp, d)
+    if old.exists():
+        shutil.rmtree(old)
     return d
 
 
-def read_config(results: Path) -> dict:
+def _state_dir(results: Path) -> Path:
+    """current_state/, or the previous complete state that a save interrupted between its two
+    renames left under current_state.old/."""
     d = Path(results) / STATE_DIR
+    old = Path(results) / (STATE_DIR + ".old")
+    return old if not d.exists() and old.exists() else d
+
+
+def read_config(results: Path) -> dict:
+    d = _state_dir(results)
     v = _name(d, "config").read_text().split()
     cfg = {"iterations": int(v[0]), "global": tuple(int(x) for x in v[1:4]), "local": tuple(int(x) for x in v[4:7]),
            "final_time": float(v[7])}
@@ -99,7 +135,7 @@ def load_state(results: Path, lat, labels: np.ndarray | None = None, ic: int = 0
     """Read results/current_state/ into case ic of `lat`: populations, macro fields and mean/rms
     sums.  Returns the config (iterations, sizes, final time, counters, stats_count).  The
     saved box must match the lattice, and the saved labels the given ones."""
-    d = Path(results) / STATE_DIR
+    d = _state_dir(results)
     cfg = read_config(results)
     nz, ny, nx = lat.shape(ic)
     if cfg["global"] != (nx, ny, nz):

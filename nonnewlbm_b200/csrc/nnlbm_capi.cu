@@ -18,7 +18,9 @@
 #include "nnlbm_kernels.cuh"
 
 namespace nnlbm {
-#define NNLBM_DECL_STEP(DT, COL) void launch_step_##DT##_##COL(bool, bool, bool, dim3, dim3, cudaStream_t, const void*);
+#define NNLBM_DECL_STEP(DT, COL)                                                                  \
+    void launch_step_##DT##_##COL(bool, bool, bool, dim3, dim3, cudaStream_t, const void*); \
+    cudaError_t load_step_##DT##_##COL();
 #define NNLBM_DECL_STEP_DT(DT)                                                                                        \
     NNLBM_DECL_STEP(DT, 0) NNLBM_DECL_STEP(DT, 1) NNLBM_DECL_STEP(DT, 2) NNLBM_DECL_STEP(DT, 3) NNLBM_DECL_STEP(DT, 4) \
     NNLBM_DECL_STEP(DT, 5) NNLBM_DECL_STEP(DT, 6) NNLBM_DECL_STEP(DT, 7) NNLBM_DECL_STEP(DT, 8) NNLBM_DECL_STEP(DT, 9) \
@@ -29,8 +31,22 @@ NNLBM_DECL_STEP_DT(0) NNLBM_DECL_STEP_DT(1) NNLBM_DECL_STEP_DT(2) NNLBM_DECL_STE
     void launch_refd_velocity_##DT(bool, dim3, dim3, cudaStream_t, const void*);         \
     void launch_refd_stress_##DT(bool, dim3, dim3, cudaStream_t, const void*);           \
     void launch_fill_eq_##DT(const void*, double, double, double, double, cudaStream_t); \
-    void launch_init_macro_##DT(const void*, double, double, double, double, cudaStream_t);
+    void launch_init_macro_##DT(const void*, double, double, double, double, cudaStream_t); \
+    cudaError_t load_bc_##DT();
 NNLBM_DECL_AUX(0) NNLBM_DECL_AUX(1) NNLBM_DECL_AUX(2) NNLBM_DECL_AUX(3)
+
+// the loaders of every kernel a launch group of (storage, collision) can launch
+static cudaError_t load_group_kernels(int dt, int col)
+{
+#define NNLBM_LROW(DT)                                                                                            \
+    {load_step_##DT##_0, load_step_##DT##_1, load_step_##DT##_2, load_step_##DT##_3, load_step_##DT##_4,         \
+     load_step_##DT##_5, load_step_##DT##_6, load_step_##DT##_7, load_step_##DT##_8, load_step_##DT##_9,         \
+     load_step_##DT##_10}
+    static cudaError_t (*const step[4][11])() = {NNLBM_LROW(0), NNLBM_LROW(1), NNLBM_LROW(2), NNLBM_LROW(3)};
+    static cudaError_t (*const bc[4])() = {load_bc_0, load_bc_1, load_bc_2, load_bc_3};
+    const cudaError_t e = step[dt][col]();
+    return e != cudaSuccess ? e : bc[dt]();
+}
 
 StepLauncher step_launcher(int dt, int col)
 {
@@ -547,11 +563,13 @@ size_t canon_index(const Case& c, int x, int y, int z, int q, int* slot)
 
 // ---------------------------------------------------------------------------------------
 // scratch of nnlbm_step_noalloc: one file-scope device array per device (the module's
-// global), never allocated or freed by this library.  Layout: [0, 256) the two step
-// cursors of the step kernels (one per A-A parity), then the gathered open-plane node values
-// (rho, ux, uy, uz per node) of the launch group being stepped.
+// global), never allocated or freed by this library.  Layout: [0, 1024) the step cursors,
+// four ints per launch group in the order of the status block (two used: one per A-A
+// parity), then the gathered open-plane node values (rho, ux, uy, uz per node) of the launch
+// group being stepped.
 // ---------------------------------------------------------------------------------------
-constexpr size_t kNoallocHead = 256;
+constexpr size_t kNoallocHead = 1024;
+constexpr size_t kNoallocGroups = kNoallocHead / (4 * sizeof(int));
 constexpr int kNoallocDevices = 64;
 std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[kNoallocDevices] = {};
@@ -563,7 +581,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NNLBM_NOALLOC_S
 namespace {
 
 // device address of the scratch array on the context's device, looked up once per device
-// with that device current (the caller has made it current)
+// with that device current (the caller has made it current).  nnlbm_create calls it, so that
+// the module holding the array is loaded then (under lazy module loading a first lookup inside
+// nnlbm_step_noalloc would load it, and allocate, there).
 int noalloc_scratch(nnlbm_ctx* ctx, char** out)
 {
     if (ctx->device < 0 || ctx->device >= kNoallocDevices)
@@ -611,13 +631,14 @@ int upload_ctl_rows(nnlbm_ctx* ctx, const Case& c, int64_t n, int flags)
     return NNLBM_OK;
 }
 
-// the group's kernel arguments with the per-call scratch moved into the static array
+// the kernel arguments of launch group gi with the per-call scratch moved into the static
+// array
 template <class CT>
-void noalloc_args(const Group& g, char* scratch, char* out)
+void noalloc_args(const Group& g, size_t gi, char* scratch, char* out)
 {
     GroupArgs<CT>& ga = *(GroupArgs<CT>*)out;
     memcpy(&ga, g.args.data(), sizeof ga);
-    ga.cursor = (int*)scratch;
+    ga.cursor = (int*)scratch + 4 * gi;
     ga.bc_buf = (CT*)(scratch + kNoallocHead);
 }
 
@@ -695,7 +716,16 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
         if (rc != NNLBM_OK) return rc;
         rebuild_case_args(ctx, c);
     }
-    return NNLBM_OK;
+    // load the kernels of every launch group and the module of nnlbm_step_noalloc's scratch
+    // now, so that no later call loads code (and allocates) on first use
+    for (const Group& g : ctx->groups) {
+        const cudaError_t e = load_group_kernels(g.dtype, g.collision);
+        if (e != cudaSuccess)
+            return set_err(ctx, NNLBM_ERR_CUDA, "loading the kernels of storage %d, collision %d failed: %s", g.dtype,
+                           g.collision, cudaGetErrorString(e));
+    }
+    char* scratch = nullptr;
+    return noalloc_scratch(ctx, &scratch);
 }
 
 int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
@@ -1102,9 +1132,12 @@ int nnlbm_import_df(nnlbm_ctx* ctx, int ic, const double* in)
                     encode(c, raw.data() + (size_t)slot * c.q_stride * eb, i, q,
                            in[(size_t)q * c.N + x + (size_t)nx * (y + (size_t)ny * z)]);
                 }
-    // on the context's stream, after whatever steps it still holds
+    // on the context's stream, after whatever steps it still holds; a new state also clears
+    // the case's watchdog flag, which reported on the state it replaces
     CK(cudaMemcpyAsync(c.df, raw.data(), raw.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(c.d_err, 0, sizeof(int), ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->status_fresh = false;
     c.has_state = true;
     return NNLBM_OK;
 }
@@ -1308,8 +1341,11 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
     char* scratch = nullptr;
     int rc = noalloc_scratch(ctx, &scratch);
     if (rc != NNLBM_OK) return rc;
+    const size_t n_groups = ctx->groups.size();
+    if (n_groups > kNoallocGroups)
+        return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: more than %zu launch groups", kNoallocGroups);
     // refuse everything that nnlbm_step would have to allocate, before any launch
-    for (size_t gi = 0; gi < ctx->groups.size(); ++gi) {
+    for (size_t gi = 0; gi < n_groups; ++gi) {
         const Group& g = ctx->groups[gi];
         if (g.dirty)
             return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: launch group %zu has no device work list yet; call "
@@ -1338,10 +1374,10 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
                                (long long)n_steps, (long long)c.ctl_cap, ic);
         }
     }
-    int cursors[64];
     ctx->status_fresh = false;
-    const size_t n_groups = ctx->groups.size();
-    if (n_groups > 64) return set_err(ctx, NNLBM_ERR_ARG, "nnlbm_step_noalloc: more than 64 launch groups");
+    // every group's cursors start at zero; the groups run one after another in stream order,
+    // so they share the node values that follow the cursors
+    CK(cudaMemsetAsync(scratch, 0, 4 * sizeof(int) * n_groups, ctx->stream));
     for (size_t gi = 0; gi < n_groups; ++gi) {
         Group& g = ctx->groups[gi];
         const bool f64 = g.dtype == NNLBM_F64;
@@ -1351,12 +1387,9 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
             if (rc != NNLBM_OK) return rc;
             if (flags & NNLBM_STEP_REDUCE) CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
         }
-        // the two cursors start at zero for every group; the group's steps, in stream
-        // order, finish before the next group clears them again
-        CK(cudaMemsetAsync(scratch, 0, 2 * sizeof(int), ctx->stream));
         alignas(64) char args[kGroupArgsBytes];
-        if (f64) noalloc_args<double>(g, scratch, args);
-        else noalloc_args<float>(g, scratch, args);
+        if (f64) noalloc_args<double>(g, gi, scratch, args);
+        else noalloc_args<float>(g, gi, scratch, args);
         const AuxLaunchers& A = aux_launchers(g.dtype);
         const int per_block = g.block / kChunk;
         const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
@@ -1372,25 +1405,20 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
             step_launcher(g.dtype, g.collision)(odd, false, g.paired, cgrid, cblk, ctx->stream, args);
         }
         CK(cudaGetLastError());
-        // pageable destination: the copy returns once the cursor is on the host; the last
-        // step stored n_steps into the cursor of the parity after it
-        CK(cudaMemcpyAsync(&cursors[gi], (int*)scratch + ((parity + n_steps) & 1), sizeof(int), cudaMemcpyDeviceToHost,
-                           ctx->stream));
         finish_steps(ctx, g, n_steps, flags);
     }
+    // the cursors into the status block, where nnlbm_step keeps them (same layout), so that the
+    // synchronous path below, or the caller's nnlbm_sync, reads them with the watchdog flags
+    CK(cudaMemcpyAsync(ctx->d_status + StatusLayout(ctx->cases.size()).cur, scratch, 4 * sizeof(int) * n_groups,
+                       cudaMemcpyDeviceToDevice, ctx->stream));
     for (Case& c : ctx->cases) {
         if (c.sched.empty()) continue;
         const int64_t rows = (int64_t)c.sched.size() / 3;
         if (n_steps < rows) c.sched.erase(c.sched.begin(), c.sched.begin() + 3 * n_steps);
         else c.sched.erase(c.sched.begin(), c.sched.end() - 3);
     }
-    // the copy of the status block waits for the cursor copies queued before it
-    if ((rc = read_status(ctx)) != NNLBM_OK) return rc;
-    for (size_t gi = 0; gi < n_groups; ++gi)
-        if (cursors[gi] != n_steps)
-            return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", gi, cursors[gi],
-                           (long long)n_steps);
-    return check_watchdog(ctx);
+    if (flags & NNLBM_STEP_ASYNC) return NNLBM_OK;
+    return wait_and_check(ctx, n_steps);
 }
 
 void* nnlbm_stream(nnlbm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

@@ -813,4 +813,26 @@ void launch_step(bool odd, bool after_gather, bool paired, dim3 grid, dim3 block
 
 StepLauncher step_launcher(int dtype, int collision);
 
+// Every variant of the step kernel of a (storage, collision) resolved now.  Under CUDA's lazy
+// module loading the runtime loads a kernel's code at its first launch, which allocates device
+// memory then; a context loads its kernels when it is created instead.
+template <int DT, int COL, bool ODD, int ARGS>
+cudaError_t load_step_variant()
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_step<DT, COL, ODD, ARGS, false>);
+    if (e == cudaSuccess && pairs_chunks(DT, COL)) e = cudaFuncGetAttributes(&fa, (const void*)k_step<DT, COL, ODD, ARGS, true>);
+    return e;
+}
+template <int DT, int COL>
+cudaError_t load_step()
+{
+    const cudaError_t e[6] = {load_step_variant<DT, COL, false, ARGS_ONE>(), load_step_variant<DT, COL, true, ARGS_ONE>(),
+                              load_step_variant<DT, COL, false, ARGS_PARAM>(), load_step_variant<DT, COL, true, ARGS_PARAM>(),
+                              load_step_variant<DT, COL, false, ARGS_GLOBAL>(), load_step_variant<DT, COL, true, ARGS_GLOBAL>()};
+    for (cudaError_t x : e)
+        if (x != cudaSuccess) return x;
+    return cudaSuccess;
+}
+
 } // namespace nnlbm

@@ -19,4 +19,6 @@ void NNLBM_CAT(launch_step_, NNLBM_DT, NNLBM_COL)(bool odd, bool after_gather, b
 {
     launch_step<NNLBM_DT, NNLBM_COL>(odd, after_gather, paired, grid, block, s, args);
 }
+
+cudaError_t NNLBM_CAT(load_step_, NNLBM_DT, NNLBM_COL)() { return load_step<NNLBM_DT, NNLBM_COL>(); }
 } // namespace nnlbm

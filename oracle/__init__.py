@@ -49,14 +49,21 @@ class _Desc(ctypes.Structure):
     ]
 
 
+def ref_dir() -> Path:
+    """The reference checkout: $NNLBM_REF_DIR, else a checkout named ``reference`` beside
+    this repository."""
+    env = os.environ.get("NNLBM_REF_DIR")
+    return Path(env) if env else HERE.parents[1] / "reference"
+
+
 def build(ref: bool | None = None) -> None:
     """Build liboracle.so, and the reference libraries when the checkout exists."""
     subprocess.check_call(["make", "-s", "-C", str(HERE), "all"])
-    ref_dir = Path(os.environ.get("NNLBM_REF_DIR", "/root/reference"))
+    rdir = ref_dir()
     if ref is None:
-        ref = (ref_dir / "solver" / "lbm3d" / "lbm_col_cum.h").exists()
+        ref = (rdir / "solver" / "lbm3d" / "core.h").exists()
     if ref:
-        subprocess.check_call(["make", "-s", "-C", str(HERE), "ref", f"NNLBM_REF_DIR={ref_dir}"])
+        subprocess.check_call(["make", "-s", "-C", str(HERE), "ref", f"NNLBM_REF_DIR={rdir}"])
 
 
 def _ptr(a: np.ndarray):
@@ -242,6 +249,7 @@ def ref_lib(fast: bool = False):
         L.ref_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ref_get_df.argtypes = [ctypes.c_void_p, _dp]
         L.ref_get_macro.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.ref_set_cy.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 4
         L.ref_set_threads.argtypes = [ctypes.c_int]
         L.ref_max_threads.restype = ctypes.c_int
         _ref[key] = L
@@ -268,14 +276,19 @@ def ref_collide(col, nu, f, rho, ux, uy, uz, fx=0.0, fy=0.0, fz=0.0, prec=8):
 
 
 class RefLattice:
-    """Single-rank reference step built from the reference headers (ref_shim.cpp)."""
+    """The reference's own step kernels (solver/lbm3d/core.h, built by ref_shim.cpp) on one
+    rank: LBMKernel alone (cy_mode CY_NONE, the deployed single-rank step) or, with
+    CY_REF_FD, the velocity / strain / step phases of the multi-rank step.  Macro fields
+    are numbered as in the C oracle (M_RHO ... M_S33)."""
 
     def __init__(self, nx, ny, nz, collision=0, equilibrium=EQ_INV_CUM_REF, nu=1.0 / 30.0,
-                 force=(0.0, 0.0, 0.0), prec=8, fast=False):
+                 force=(0.0, 0.0, 0.0), prec=8, fast=False, cy_mode=CY_NONE, cy=(0.0, 0.0, 2.0, 1.0)):
         self.L = ref_lib(fast)
         self.h = self.L.ref_create(prec, nx, ny, nz, collision, equilibrium, nu, *force)
         if not self.h:
             raise ValueError("bad reference lattice parameters")
+        if cy_mode != CY_NONE and self.L.ref_set_cy(self.h, cy_mode, *cy) != 0:
+            raise ValueError("the reference has no Carreau-Yasuda mode %d" % cy_mode)
         self.shape = (nz, ny, nx)
         self.N = nx * ny * nz
 
@@ -311,5 +324,6 @@ class RefLattice:
 
     def get_macro(self, field):
         a = np.zeros(self.N)
-        self.L.ref_get_macro(self.h, field, _ptr(a))
+        if self.L.ref_get_macro(self.h, field, _ptr(a)) != 0:
+            raise ValueError(f"bad macro field {field}")
         return a.reshape(self.shape)

@@ -1,77 +1,176 @@
-// ref_shim.cpp -- builds the reference's own collision, equilibrium, streaming and generic
-// boundary-condition headers (solver/lbm3d/*.h of buresjan/nonnewlbm, included unmodified
-// from the reference checkout) into oracle/_ref/libnnlbm_ref.so.
+// ref_shim.cpp -- the reference's own per-cell kernels of solver/lbm3d/core.h (buresjan/nonnewlbm),
+// compiled unmodified on the host into oracle/_ref/libnnlbm_ref.so (FP64 parity build) and
+// oracle/_ref/libnnlbm_ref_fast.so (timing build).
 //
-// TEST INFRASTRUCTURE ONLY: used to pin the C oracle (known-answer vectors under
-// tests/golden/) and, in its single-precision build, as the timed CPU baseline of
-// bench.py.  Nothing in the product links it.
+// TEST INFRASTRUCTURE ONLY: it pins the C oracle (known-answer vectors under tests/golden/),
+// is compared with the GPU step directly by the GPU tests, and its single-precision build is
+// the timed CPU baseline of bench.py.  Nothing in the product links it.
 //
-// The reference's defs.h cannot be included (it pulls TNL, libpng and MPI), so this file
-// declares the few interface types those headers expect: the CUDA_HOSTDEV macros, the
-// df_cur/df_out enum, the 27-direction enum and a KernelStruct with the member names the
-// headers use (solver/lbm3d/defs.h:26-40,143-160,215-247).  The kernel driver at the end
-// is a restatement of the single-rank host loop (solver/lbm3d/core.h:1312-1320) around
-// LBMKernel (core.h:578-800) and the TCPC policies (solver/sim_tcpc/sim_tcpc.cu:187-354),
-// calling the reference templates for every per-cell operation.
-#include <cmath>
+// core.h is included as it ships.  Its own #include "defs.h" / "state.h" / "lbm.h" land on
+// the stand-ins of oracle/ref_stub/ (oracle/Makefile searches that directory first, with
+// -I-), which declare the interface types those headers take from TNL-bound code.  Every
+// per-cell operation therefore runs the reference's code: LBMKernel (core.h:578-800) with its
+// finite-difference Carreau-Yasuda force, the multi-rank pre-kernels LBMKernelVelocity
+// (core.h:273-384) and LBMKernelStress (core.h:387-576), LBMKernelInit (core.h:833-863), the
+// streaming, collision and equilibrium templates, the generic boundary blocks of lbm_bc.h and
+// MacroDefault of lbm_macro.h.  Written here are only what sim_tcpc.cu and TNL would supply:
+//   ShimData  the LBM_DATA policy over plain arrays (index map y + Y*(z + Z*(q + 27*x)) of
+//             solver/lbm3d/lbm_data.h:61-71) with LBM_Data_Tcpc's inflow rules
+//             (sim_tcpc.cu:281-320) and the per-cell inflow of LBM_Data_ConstInflow
+//             (lbm_data.h:352-367);
+//   ShimBC    the LBM_BC policy: the predicates and BC switch of LBM_BC_Tcpc
+//             (sim_tcpc.cu:187-279), which lives in sim_tcpc.cu next to its main() and VTK
+//             reader and cannot be included, extended by the generic GEO_INFLOW and
+//             GEO_OUTFLOW_RIGHT_EQ blocks, which it takes from LBM_BC_All (lbm_bc.h:126-152);
+//   the loops: the host loop of core.h:1312-1320 (x, z, y order, collapse(2)) around each
+//             kernel, and for the finite-difference Carreau-Yasuda mode the three phases of
+//             the multi-rank step (core.h:1169-1310) on one rank, with the pointer swap of
+//             lbm.hpp:392-418 after each step.
+#include <algorithm>
 #include <cstdint>
-#include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <algorithm>
-#include <utility>
+#include <vector>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
 
-#define CUDA_HOSTDEV
-#define CUDA_HOSTDEV_NOINLINE
-#define USE_CYMODEL
-
-enum : uint8_t { df_cur, df_out, DFMAX };
-
-enum {
-    mmm = 0, mmz, mmp, mzm, mzz, mzp, mpm, mpz, mpp,
-    zmm, zmz, zmp, zzm, zzz, zzp, zpm, zpz, zpp,
-    pmm, pmz, pmp, pzm, pzz, pzp, ppm, ppz, ppp
-};
-
-template <typename REAL>
-struct KernelStruct {
-    REAL fz = 0, fx = 0, fy = 0;
-    REAL f[27];
-    REAL vz = 0, vx = 0, vy = 0, rho = 1.0, lbmViscosity = 1.0;
-    REAL S11 = 0., S12 = 0., S22 = 0., S32 = 0., S13 = 0., S33 = 0.;
-    REAL lbm_nu0 = 0, lbm_lambda = 0, lbm_a = 0, lbm_n = 0;
-    REAL mu;
-};
-
-template <typename DREAL>
-struct ShimTraits {
-    using real = double;
-    using dreal = DREAL;
-    using idx = long;
-    using map_t = short;
-};
-
-#include "ciselnik.h"
-#include "lbm_eq.h"
-#include "lbm_eq_inv_cum.h"
-#include "lbm_eq_entropic.h"
-#include "lbm_common.h"
-#include "lbm_streaming.h"
-#include "lbm_col_cum.h"
-#include "lbm_col_mrt.h"
-#include "lbm_col_bgk.h"
-#include "lbm_col_kbc_n.h"
-#include "lbm_col_kbc_c.h"
-#include "lbm_bc.h"
+#include "core.h"
 
 namespace {
 
-// equilibrium selector: 0 = LBM_EQ_INV_CUM (as shipped), 2 = LBM_EQ_DEFAULT,
-// 3 = LBM_EQ_ENTROPIC.  (1, the corrected factorised equilibrium, has no reference
-// counterpart and is not provided here.)
+// solver map labels of this repository: 0..6 are LBM_BC_Tcpc::GEO (sim_tcpc.cu:194-203); 7 and 8
+// stand for LBM_BC_All's GEO_INFLOW and GEO_OUTFLOW_RIGHT_EQ
+enum { L_FLUID = 0, L_WALL = 1, L_PERIODIC = 2, L_IN_L = 3, L_IN_R = 4, L_OUT_F = 5, L_OUT_B = 6, L_IN_EQ = 7, L_OUT_REQ = 8 };
+enum { CY_NONE = 0, CY_REF_FD = 1 };
+
+template <typename T>
+using ShimTraits = Traits<T, double, long, short>;
+
+// LBM_DATA policy over plain host arrays
+template <typename T>
+struct ShimData {
+    T* dfs[DFMAX];
+    T* mac;                 // [MacroDefault::N][N], x fastest
+    const uint8_t* lab;     // [N] labels, x fastest
+    const double* prof;     // [3][N] prescribed velocity of L_IN_EQ cells
+    long X_, Y_, Z_, N_;
+    T lbmViscosity = 1, fx = 0, fy = 0, fz = 0;
+    T lbm_nu0 = 0, lbm_lambda = 0, lbm_a = 1, lbm_n = 1;
+    T inflow_rho_left = 1, inflow_rho_right = 1, inflow_rho_eq = 1;
+    T inflow_left = 0, inflow_right = 0;
+    long inflow_left_area = 0, inflow_right_area = 0;
+
+    long X() const { return X_; }
+    long Y() const { return Y_; }
+    long Z() const { return Z_; }
+    long cell(long x, long y, long z) const { return x + X_ * (y + Y_ * z); }
+    T& df(uint8_t type, int q, long x, long y, long z) { return dfs[type][y + Y_ * (z + Z_ * (q + 27 * x))]; }
+    short map(long x, long y, long z) const { return (short)lab[cell(x, y, z)]; }
+    T& macro(int id, long x, long y, long z) { return mac[(long)id * N_ + cell(x, y, z)]; }
+
+    // LBM_Data_Tcpc::inflowCondition{Left,Right} (sim_tcpc.cu:295-309)
+    void inflowConditionLeft(KernelStruct<T>& KS, long, long, long)
+    {
+        KS.rho = inflow_rho_left;
+        KS.vx = inflow_left_area > 0 ? inflow_left / (T)inflow_left_area : (T)0;
+        KS.vy = (T)0;
+        KS.vz = (T)0;
+    }
+    void inflowConditionRight(KernelStruct<T>& KS, long, long, long)
+    {
+        KS.rho = inflow_rho_right;
+        KS.vx = inflow_right_area > 0 ? inflow_right / (T)inflow_right_area : (T)0;
+        KS.vy = (T)0;
+        KS.vz = (T)0;
+    }
+    // LBM_Data_Tcpc::inflow (sim_tcpc.cu:311-319) for the two TCPC planes; the prescribed
+    // per-cell velocity (LBM_Data_ConstInflow) for GEO_INFLOW cells
+    void inflow(KernelStruct<T>& KS, long x, long y, long z)
+    {
+        const int l = map(x, y, z);
+        if (l == L_IN_R) { inflowConditionRight(KS, x, y, z); return; }
+        if (l == L_IN_L) { inflowConditionLeft(KS, x, y, z); return; }
+        const long c = cell(x, y, z);
+        KS.rho = inflow_rho_eq;
+        KS.vx = (T)prof[c];
+        KS.vy = (T)prof[N_ + c];
+        KS.vz = (T)prof[2 * N_ + c];
+    }
+};
+
+// LBM_BC policy: LBM_BC_Tcpc's predicates and switch plus the two generic blocks
+template <typename TRAITS>
+struct ShimBC {
+    using dreal = typename TRAITS::dreal;
+    using idx = typename TRAITS::idx;
+    using map_t = typename TRAITS::map_t;
+    using G = LBM_BC_All<TRAITS>;
+
+    static bool isPeriodic(map_t m) { return m == L_PERIODIC; }
+    static bool isFluid(map_t m) { return m == L_FLUID; }
+    static bool isNotFluid(map_t m) { return m != L_FLUID; }
+    static bool isWall(map_t m) { return m == L_WALL; }
+    static bool isInflow(map_t m) { return m == L_IN_L || m == L_IN_R || m == L_IN_EQ; }
+    static bool isOutflowR(map_t m) { return m == L_OUT_F || m == L_OUT_B || m == L_OUT_REQ; }
+    static bool isStreaming(map_t m) { return m == L_FLUID || m == L_PERIODIC; }
+    static bool isComputeDensityAndVelocity(map_t m) { return m == L_FLUID || m == L_PERIODIC; }
+
+    template <typename L, typename S, typename LBM_DATA>
+    static bool BC(LBM_DATA& SD, KernelStruct<dreal>& KS, idx m, idx xm, idx x, idx xp, idx ym, idx y, idx yp, idx zm,
+                   idx z, idx zp)
+    {
+        switch (m) {
+        case L_WALL: // sim_tcpc.cu:235-241
+            S::streamingBounceBack(SD, KS, xm, x, xp, ym, y, yp, zm, z, zp);
+            KS.rho = no1;
+            KS.vx = KS.vy = KS.vz = (dreal)0;
+            return true;
+        case L_IN_L:
+        case L_IN_R: { // sim_tcpc.cu:242-261: rho of the post-streaming state one cell inward
+            if (m == L_IN_L) SD.inflowConditionLeft(KS, x, y, z);
+            else SD.inflowConditionRight(KS, x, y, z);
+            KernelStruct<dreal> inward;
+            if (m == L_IN_L) S::streaming(SD, inward, x, xp, xp + 1, ym, y, yp, zm, z, zp);
+            else S::streaming(SD, inward, xm - 1, xm, x, ym, y, yp, zm, z, zp);
+            L::computeDensityAndVelocity(inward);
+            KS.rho = inward.rho;
+            L::setEquilibrium(KS);
+            return true;
+        }
+        case L_OUT_F:
+        case L_OUT_B: // sim_tcpc.cu:262-273: velocity one cell inward, rho = 1
+            if (m == L_OUT_F) S::streaming(SD, KS, xm, x, xp, y, yp, yp + 1, zm, z, zp);
+            else S::streaming(SD, KS, xm, x, xp, ym - 1, ym, y, zm, z, zp);
+            L::computeDensityAndVelocity(KS);
+            KS.rho = no1;
+            L::setEquilibrium(KS);
+            return true;
+        case L_IN_EQ:
+            return G::template BC<L, S, LBM_DATA>(SD, KS, G::GEO_INFLOW, xm, x, xp, ym, y, yp, zm, z, zp);
+        case L_OUT_REQ:
+            return G::template BC<L, S, LBM_DATA>(SD, KS, G::GEO_OUTFLOW_RIGHT_EQ, xm, x, xp, ym, y, yp, zm, z, zp);
+        default:
+            return false;
+        }
+    }
+};
+
+// LBMKernelInit's view of the lattice (core.h:839-863): the map, the host populations and
+// the kernel data
+template <typename T>
+struct ShimHostDF {
+    const T* a;
+    long Y, Z;
+    T operator()(int q, long x, long y, long z) const { return a[y + Y * (z + Z * (q + 27 * x))]; }
+};
+template <typename T>
+struct ShimLBM {
+    ShimData<T> data;
+    ShimHostDF<T> hfs[DFMAX];
+    short map(long x, long y, long z) const { return data.map(x, y, z); }
+};
+
 template <typename T, int EQ> struct EqSel;
 template <typename T> struct EqSel<T, 0> { using type = LBM_EQ_INV_CUM<ShimTraits<T>>; };
 template <typename T> struct EqSel<T, 2> { using type = LBM_EQ_DEFAULT<ShimTraits<T>>; };
@@ -90,143 +189,52 @@ template <typename T, typename EQ> struct ColSel<T, 8, EQ> { using type = LBM_KB
 template <typename T, typename EQ> struct ColSel<T, 9, EQ> { using type = LBM_MRT<ShimTraits<T>, EQ>; };
 template <typename T, typename EQ> struct ColSel<T, 10, EQ> { using type = LBM_BGK<ShimTraits<T>, EQ>; };
 
-// ---------------------------------------------------------------------------------
-// lattice data adaptor with the reference index map y + Y*(z + Z*(q + 27*x))
-// (solver/lbm3d/lbm_data.h:296-312)
-// ---------------------------------------------------------------------------------
-template <typename T>
-struct ShimData {
-    T* dfs[DFMAX];
-    long X_, Y_, Z_;
-    long X() const { return X_; }
-    long Y() const { return Y_; }
-    long Z() const { return Z_; }
-    T& df(uint8_t type, int q, long x, long y, long z) { return dfs[type][y + Y_ * (z + Z_ * (q + 27 * x))]; }
-    // inflow data (LBM_Data_Tcpc, sim_tcpc.cu:288-309; generic per-cell inflow)
-    T inflow_left = 0, inflow_right = 0, inflow_rho_left = 1, inflow_rho_right = 1, inflow_rho_eq = 1;
-    long inflow_left_area = 0, inflow_right_area = 0;
-    const double* prof = nullptr; // [3][N], N over x fastest
-    void inflowConditionLeft(KernelStruct<T>& KS, long, long, long)
-    {
-        KS.rho = inflow_rho_left;
-        KS.vx = inflow_left_area > 0 ? inflow_left / (T)inflow_left_area : (T)0;
-        KS.vy = (T)0;
-        KS.vz = (T)0;
-    }
-    void inflowConditionRight(KernelStruct<T>& KS, long, long, long)
-    {
-        KS.rho = inflow_rho_right;
-        KS.vx = inflow_right_area > 0 ? inflow_right / (T)inflow_right_area : (T)0;
-        KS.vy = (T)0;
-        KS.vz = (T)0;
-    }
-    void inflow(KernelStruct<T>& KS, long x, long y, long z)
-    {
-        long c = x + X_ * (y + Y_ * z), N = X_ * Y_ * Z_;
-        KS.rho = inflow_rho_eq;
-        KS.vx = (T)prof[c];
-        KS.vy = (T)prof[N + c];
-        KS.vz = (T)prof[2 * N + c];
-    }
-};
-
-enum { L_FLUID = 0, L_WALL = 1, L_PERIODIC = 2, L_IN_L = 3, L_IN_R = 4, L_OUT_F = 5, L_OUT_B = 6, L_IN_EQ = 7, L_OUT_REQ = 8 };
+using MacroF = MacroDefault<ShimTraits<float>>;
+// macro fields in the C oracle's numbering (oracle/nnlbm_oracle.h), as MacroDefault ids
+const int kMacroOf[20] = {MacroF::e_rho, MacroF::e_vx, MacroF::e_vy, MacroF::e_vz,
+                          MacroF::e_vm_plus_x, MacroF::e_vm_minus_x, MacroF::e_vm_y, MacroF::e_vm_z,
+                          MacroF::e_vm_xx, MacroF::e_vm_yy, MacroF::e_vm_zz,
+                          MacroF::e_fx, MacroF::e_fy, MacroF::e_fz,
+                          MacroF::e_S11, MacroF::e_S12, MacroF::e_S13, MacroF::e_S22, MacroF::e_S32, MacroF::e_S33};
+// the mean/rms sums, which MacroDefault::outputMacro adds to on every call
+const int kStatFields[7] = {MacroF::e_vm_plus_x, MacroF::e_vm_minus_x, MacroF::e_vm_y, MacroF::e_vm_z,
+                            MacroF::e_vm_xx, MacroF::e_vm_yy, MacroF::e_vm_zz};
 
 struct Lattice {
     int prec; // 8 or 4
-    int col, eq;
+    int col, eq, cy_mode = CY_NONE;
     long X, Y, Z, N;
     double nu, fx, fy, fz;
+    double nu0 = 0, lam = 0, a = 1, n = 1;
     uint8_t* map;
     void* df[2];
     int cur;
     double* prof;
-    void* macro; // [7 + 7 stats][N]: rho vx vy vz fx fy fz | vm+x vm-x vmy vmz vmxx vmyy vmzz
+    void* macro; // [MacroDefault::N][N]
     double ivc_flux = 0, svc_flux = 0, rho_l = 1, rho_r = 1, rho_eq = 1;
     long left_area = 0, right_area = 0;
 };
 
-template <typename T, typename LT>
-void cell_step(Lattice& L, ShimData<T>& SD, T* macro, long x, long y, long z, int acc)
-{
-    using S = LBM_STREAMING<ShimTraits<T>>;
-    using BCG = LBM_BC_All<ShimTraits<T>>;
-    using dreal = T;
-    const long c = x + L.X * (y + L.Y * z);
-    const int lab = L.map[c];
-    KernelStruct<T> KS;
-    KS.lbmViscosity = (T)L.nu;
-    KS.fx = (T)L.fx; KS.fy = (T)L.fy; KS.fz = (T)L.fz;
-    long xp, xm, yp, ym, zp, zm;
-    if (lab == L_PERIODIC) {
-        xp = x == L.X - 1 ? 0 : x + 1; xm = x == 0 ? L.X - 1 : x - 1;
-        yp = y == L.Y - 1 ? 0 : y + 1; ym = y == 0 ? L.Y - 1 : y - 1;
-        zp = z == L.Z - 1 ? 0 : z + 1; zm = z == 0 ? L.Z - 1 : z - 1;
-    } else {
-        xp = std::min(x + 1, L.X - 1); xm = std::max(x - 1, 0L);
-        yp = std::min(y + 1, L.Y - 1); ym = std::max(y - 1, 0L);
-        zp = std::min(z + 1, L.Z - 1); zm = std::max(z - 1, 0L);
-    }
-    if (lab == L_FLUID || lab == L_PERIODIC) {
-        S::streaming(SD, KS, xm, x, xp, ym, y, yp, zm, z, zp);
-        LT::computeDensityAndVelocity(KS);
-        LT::collision(KS);
-    } else if (lab == L_WALL) {
-        BCG::template BC<LT, S, ShimData<T>>(SD, KS, BCG::GEO_WALL, xm, x, xp, ym, y, yp, zm, z, zp);
-    } else if (lab == L_IN_L) {
-        SD.inflowConditionLeft(KS, x, y, z);
-        KernelStruct<T> KS_loc;
-        S::streaming(SD, KS_loc, x, xp, xp + 1, ym, y, yp, zm, z, zp);
-        LT::computeDensityAndVelocity(KS_loc);
-        KS.rho = KS_loc.rho;
-        LT::setEquilibrium(KS);
-    } else if (lab == L_IN_R) {
-        SD.inflowConditionRight(KS, x, y, z);
-        KernelStruct<T> KS_loc;
-        S::streaming(SD, KS_loc, xm - 1, xm, x, ym, y, yp, zm, z, zp);
-        LT::computeDensityAndVelocity(KS_loc);
-        KS.rho = KS_loc.rho;
-        LT::setEquilibrium(KS);
-    } else if (lab == L_OUT_F) {
-        S::streaming(SD, KS, xm, x, xp, y, yp, yp + 1, zm, z, zp);
-        LT::computeDensityAndVelocity(KS);
-        KS.rho = no1;
-        LT::setEquilibrium(KS);
-    } else if (lab == L_OUT_B) {
-        S::streaming(SD, KS, xm, x, xp, ym - 1, ym, y, zm, z, zp);
-        LT::computeDensityAndVelocity(KS);
-        KS.rho = no1;
-        LT::setEquilibrium(KS);
-    } else if (lab == L_IN_EQ) {
-        // GEO_INFLOW streams first (isStreaming) and then overwrites everything
-        BCG::template BC<LT, S, ShimData<T>>(SD, KS, BCG::GEO_INFLOW, xm, x, xp, ym, y, yp, zm, z, zp);
-    } else if (lab == L_OUT_REQ) {
-        S::streaming(SD, KS, xm, x, xp, ym, y, yp, zm, z, zp);
-        LT::computeDensityAndVelocity(KS);
-        BCG::template BC<LT, S, ShimData<T>>(SD, KS, BCG::GEO_OUTFLOW_RIGHT_EQ, xm, x, xp, ym, y, yp, zm, z, zp);
-    }
-    LT::copyKS2DFout(SD, KS, x, y, z);
-    const long N = L.N;
-    macro[0 * N + c] = KS.rho; macro[1 * N + c] = KS.vx; macro[2 * N + c] = KS.vy; macro[3 * N + c] = KS.vz;
-    macro[4 * N + c] = KS.fx; macro[5 * N + c] = KS.fy; macro[6 * N + c] = KS.fz;
-    if (acc) {
-        macro[7 * N + c] += (KS.vx > 0) ? KS.rho * KS.vx : 0;
-        macro[8 * N + c] += (KS.vx < 0) ? KS.rho * KS.vx : 0;
-        macro[9 * N + c] += KS.rho * KS.vy;
-        macro[10 * N + c] += KS.rho * KS.vz;
-        macro[11 * N + c] += KS.rho * KS.rho * KS.vx * KS.vx;
-        macro[12 * N + c] += KS.rho * KS.rho * KS.vy * KS.vy;
-        macro[13 * N + c] += KS.rho * KS.rho * KS.vz * KS.vz;
-    }
-}
-
-template <typename T, typename LT>
-void lattice_step(Lattice& L, int acc)
+template <typename T>
+ShimData<T> make_data(Lattice& L)
 {
     ShimData<T> SD;
     SD.dfs[df_cur] = (T*)L.df[L.cur];
     SD.dfs[df_out] = (T*)L.df[1 - L.cur];
-    SD.X_ = L.X; SD.Y_ = L.Y; SD.Z_ = L.Z;
+    SD.mac = (T*)L.macro;
+    SD.lab = L.map;
+    SD.prof = L.prof;
+    SD.X_ = L.X; SD.Y_ = L.Y; SD.Z_ = L.Z; SD.N_ = L.N;
+    SD.lbmViscosity = (T)L.nu;
+    SD.fx = (T)L.fx; SD.fy = (T)L.fy; SD.fz = (T)L.fz;
+    if (L.cy_mode == CY_REF_FD) {
+        SD.lbm_nu0 = (T)L.nu0; SD.lbm_lambda = (T)L.lam; SD.lbm_a = (T)L.a; SD.lbm_n = (T)L.n;
+    } else {
+        // a Newtonian law: with the zero strain of the single-rank step the force term of
+        // core.h:779-781 is exactly zero, as in the deployed sim_tcpc
+        SD.lbm_nu0 = (T)L.nu; SD.lbm_lambda = 0; SD.lbm_a = 1; SD.lbm_n = 1;
+    }
+    // sim_tcpc.cu:657-663: inflow_right = -svc_flux
     SD.inflow_left = (T)L.ivc_flux;
     SD.inflow_right = (T)(-L.svc_flux);
     SD.inflow_rho_left = (T)L.rho_l;
@@ -234,19 +242,46 @@ void lattice_step(Lattice& L, int acc)
     SD.inflow_rho_eq = (T)L.rho_eq;
     SD.inflow_left_area = L.left_area;
     SD.inflow_right_area = L.right_area;
-    SD.prof = L.prof;
-    T* macro = (T*)L.macro;
-    // core.h:1313-1320 loop order
-#pragma omp parallel for schedule(static) collapse(2) firstprivate(SD)
+    return SD;
+}
+
+// the host loop of core.h:1312-1320 around one kernel
+template <typename F>
+void for_cells(const Lattice& L, F&& body)
+{
+#pragma omp parallel for schedule(static) collapse(2)
     for (long x = 0; x < L.X; x++)
         for (long z = 0; z < L.Z; z++)
-            for (long y = 0; y < L.Y; y++) cell_step<T, LT>(L, SD, macro, x, y, z, acc);
-    L.cur = 1 - L.cur;
+            for (long y = 0; y < L.Y; y++) body(x, y, z);
+}
+
+template <typename T, typename LT>
+void lattice_step(Lattice& L, int acc)
+{
+    using TR = ShimTraits<T>;
+    using S = LBM_STREAMING<TR>;
+    using M = MacroDefault<TR>;
+    using D = ShimData<T>;
+    using BC = ShimBC<TR>;
+    const D SD = make_data<T>(L);
+    T* mac = (T*)L.macro;
+    std::vector<T> keep;
+    if (!acc) keep.assign(mac + (long)kStatFields[0] * L.N, mac + (long)(kStatFields[6] + 1) * L.N);
+    if (L.cy_mode == CY_REF_FD) {
+        // core.h:1169-1258 on one rank: the velocity of the post-streaming state, then the
+        // finite-difference strain, then the step with the force of that strain
+        for_cells(L, [&](long x, long y, long z) { LBMKernelVelocity<LT, S, M, D, BC>(SD, x, y, z, 0, 1); });
+        for_cells(L, [&](long x, long y, long z) { LBMKernelStress<LT, S, M, D, BC>(SD, x, y, z, 0, 1); });
+    }
+    for_cells(L, [&](long x, long y, long z) { LBMKernel<LT, S, M, D, BC>(SD, x, y, z, 0, 1); });
+    if (!acc) std::copy(keep.begin(), keep.end(), mac + (long)kStatFields[0] * L.N);
+    L.cur = 1 - L.cur; // lbm.hpp:392-418
 }
 
 template <typename T, typename LT>
 void lattice_init(Lattice& L, double rho, double vx, double vy, double vz)
 {
+    // resetLattice / setEqLat (sim_tcpc.cu:647-655, lbm.hpp:1-39): both lattices at feq
     KernelStruct<T> KS;
     KS.rho = (T)rho; KS.vx = (T)vx; KS.vy = (T)vy; KS.vz = (T)vz;
     LT::setEquilibrium(KS);
@@ -258,6 +293,18 @@ void lattice_init(Lattice& L, double rho, double vx, double vy, double vz)
                     for (long y = 0; y < L.Y; ++y) a[y + L.Y * (z + L.Z * (q + 27 * x))] = KS.f[q];
     }
     L.cur = 0;
+    // the initial macro fields (LBMKernelInit over every cell, core.h:1531-1536); its call of
+    // outputMacro also adds the initial state to the mean/rms sums, which start at zero here
+    using TR = ShimTraits<T>;
+    using M = MacroDefault<TR>;
+    using BC = ShimBC<TR>;
+    memset(L.macro, 0, (size_t)L.N * M::N * L.prec);
+    ShimLBM<T> lbm;
+    lbm.data = make_data<T>(L);
+    lbm.hfs[df_cur] = {(const T*)L.df[L.cur], L.Y, L.Z};
+    lbm.hfs[df_out] = {(const T*)L.df[1 - L.cur], L.Y, L.Z};
+    for_cells(L, [&](long x, long y, long z) { LBMKernelInit<LT, BC, M, ShimLBM<T>>(lbm, x, y, z); });
+    for (int f : kStatFields) memset((T*)L.macro + (long)f * L.N, 0, (size_t)L.N * sizeof(T));
 }
 
 template <typename T, int COL, int EQ>
@@ -371,7 +418,8 @@ int ref_collide(int prec, int col, double nu, double* f, double rho, double vx, 
 // lattice: map labels 0..8 as in the C oracle; df exported as [27][N], x fastest
 void* ref_create(int prec, int nx, int ny, int nz, int col, int eq, double nu, double fx, double fy, double fz)
 {
-    if (nx < 3 || ny < 3 || nz < 3 || (prec != 4 && prec != 8)) return nullptr;
+    if (nx < 3 || ny < 3 || nz < 3 || (prec != 4 && prec != 8) || col < 0 || col > 10 || (eq != 0 && eq != 2 && eq != 3))
+        return nullptr;
     Lattice* L = new Lattice();
     L->prec = prec; L->col = col; L->eq = eq;
     L->X = nx; L->Y = ny; L->Z = nz; L->N = (long)nx * ny * nz;
@@ -379,10 +427,21 @@ void* ref_create(int prec, int nx, int ny, int nz, int col, int eq, double nu, d
     L->map = (uint8_t*)calloc(L->N, 1);
     L->df[0] = calloc(L->N * 27, prec);
     L->df[1] = calloc(L->N * 27, prec);
-    L->macro = calloc(L->N * 14, prec);
+    L->macro = calloc(L->N * MacroF::N, prec);
     L->prof = (double*)calloc(L->N * 3, sizeof(double));
     L->cur = 0;
     return L;
+}
+
+// Carreau-Yasuda coupling: 0 = none (the deployed single-rank step), 1 = the
+// finite-difference force of the multi-rank step; lattice-unit nu0, lambda, a, n
+int ref_set_cy(void* h, int mode, double nu0, double lam, double a, double n)
+{
+    Lattice* L = (Lattice*)h;
+    if (mode != CY_NONE && mode != CY_REF_FD) return -1;
+    if (mode == CY_REF_FD && !(a > 0)) return -1;
+    L->cy_mode = mode; L->nu0 = nu0; L->lam = lam; L->a = a; L->n = n;
+    return 0;
 }
 
 void ref_destroy(void* h)
@@ -421,7 +480,6 @@ int ref_init(void* h, double rho, double vx, double vy, double vz)
 {
     Lattice* L = (Lattice*)h;
     double a[4] = {rho, vx, vy, vz};
-    memset(L->macro, 0, L->N * 14 * L->prec);
     return run(L->prec, L->col, L->eq, 1, L, 0, a, nullptr);
 }
 
@@ -444,11 +502,16 @@ void ref_get_df(void* h, double* out)
                 }
 }
 
-void ref_get_macro(void* h, int field, double* out)
+// one macro field, numbered as in the C oracle (oracle/nnlbm_oracle.h: rho vx vy vz, the
+// seven mean/rms sums, fx fy fz, S11 S12 S13 S22 S32 S33)
+int ref_get_macro(void* h, int field, double* out)
 {
     Lattice* L = (Lattice*)h;
+    if (field < 0 || field >= 20) return -1;
+    const long off = (long)kMacroOf[field] * L->N;
     for (long c = 0; c < L->N; ++c)
-        out[c] = L->prec == 4 ? (double)((float*)L->macro)[field * L->N + c] : ((double*)L->macro)[field * L->N + c];
+        out[c] = L->prec == 4 ? (double)((float*)L->macro)[off + c] : ((double*)L->macro)[off + c];
+    return 0;
 }
 
 void ref_set_threads(int n)

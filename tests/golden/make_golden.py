@@ -1,8 +1,10 @@
 """Generate the golden known-answer fixtures of tests/golden/ from the reference itself.
 
-Every expected value here is computed by the reference's own headers (solver/lbm3d/*.h of
-buresjan/nonnewlbm, compiled unmodified into oracle/_ref/libnnlbm_ref.so by
-oracle/Makefile) in FP64, on seeded inputs.  The reference ships no tests or fixtures of
+Every expected value here is computed by the reference's own code in FP64, on seeded
+inputs: the per-cell headers (solver/lbm3d/*.h of buresjan/nonnewlbm) and, for the lattice
+cases, the step kernels of solver/lbm3d/core.h (LBMKernel, and for the finite-difference
+Carreau-Yasuda cases LBMKernelVelocity and LBMKernelStress before it), all compiled
+unmodified into oracle/_ref/libnnlbm_ref.so by oracle/Makefile.  The reference ships no tests or fixtures of
 its own, so these vectors are what pins the C oracle.  Run in a container that has the
 reference checkout:
 
@@ -52,9 +54,10 @@ def per_cell(rng):
                         eq_out=eq_out)
 
 
-def lattice_case(name, labels, col, eq, nu, steps, inflow=None, profile=None, force=(0.0, 0.0, 0.0)):
+def lattice_case(name, labels, col, eq, nu, steps, inflow=None, profile=None, force=(0.0, 0.0, 0.0),
+                 cy_mode=O.CY_NONE, cy=(0.0, 0.0, 2.0, 1.0)):
     nz, ny, nx = labels.shape
-    ref = O.RefLattice(nx, ny, nz, collision=col, equilibrium=eq, nu=nu, force=force)
+    ref = O.RefLattice(nx, ny, nz, collision=col, equilibrium=eq, nu=nu, force=force, cy_mode=cy_mode, cy=cy)
     ref.set_map(labels)
     if inflow is not None:
         ref.set_inflow(*inflow)
@@ -62,9 +65,10 @@ def lattice_case(name, labels, col, eq, nu, steps, inflow=None, profile=None, fo
         ref.set_inflow_profile(profile)
     ref.init_equilibrium()
     ref.step(steps)
-    macro = np.stack([ref.get_macro(k) for k in range(14)])
+    # every macro field, numbered as in the C oracle (M_RHO ... M_S33)
+    macro = np.stack([ref.get_macro(k) for k in range(20)])
     np.savez_compressed(HERE / f"{name}.npz", labels=labels, df=ref.get_df(), macro=macro,
-                        meta=np.array([col, eq, nu, steps, *force]),
+                        meta=np.array([col, eq, nu, steps, *force]), cy=np.array([cy_mode, *cy], dtype=float),
                         inflow=np.array(inflow if inflow is not None else [0, 0, 1, 1, 1], dtype=float),
                         profile=profile if profile is not None else np.zeros(0))
 
@@ -89,6 +93,12 @@ def main():
     lattice_case("step_tcpc_kbc_c4", labels, O.COLLISIONS.index("KBC_C4"), O.EQ_ENTROPIC, 0.02, 30, inflow=inflow)
     lattice_case("step_tcpc_bgk_force", labels, O.COLLISIONS.index("BGK"), O.EQ_DEFAULT, 0.02, 30, inflow=inflow,
                  force=(1e-5, -2e-5, 5e-6))
+    # the finite-difference Carreau-Yasuda coupling of the multi-rank step (core.h:273-800)
+    cy = (0.05, 40.0, 2.0, 0.3568)  # nu0, lambda, a, n in lattice units (nu_inf = 0.02)
+    lattice_case("step_tcpc_cum_reffd", labels, O.COLLISIONS.index("CUM"), O.EQ_INV_CUM_REF, 0.02, 30, inflow=inflow,
+                 cy_mode=O.CY_REF_FD, cy=cy)
+    lattice_case("step_tcpc_bgk_reffd", labels, O.COLLISIONS.index("BGK"), O.EQ_DEFAULT, 0.02, 30, inflow=inflow,
+                 force=(1e-5, -2e-5, 5e-6), cy_mode=O.CY_REF_FD, cy=cy)
     m, prof = G.pipe_map(16, 9, 9, 3.2)
     lattice_case("step_pipe_mrt", m, O.COLLISIONS.index("MRT_LES"), O.EQ_INV_CUM_REF, 1.0 / 30.0, 30,
                  profile=G.expand_profile(m, prof) * 0.04)

@@ -103,3 +103,31 @@ def test_driver_flags(tmp_path):
     r2.load_state(cnt2)
     assert r2.iterations == 55 and cnt2["vtk"].count == 4 and r2.prev_iter == 55 - r.lat.n
     assert np.array_equal(r2.lat.df, r.lat.df)
+
+
+def test_interrupted_save_keeps_the_previous_state(tmp_path):
+    """A save that dies before its files are complete leaves the last complete state in
+    place (files go to a sibling directory and are swapped in at the end)."""
+    labels = np.arange(60, dtype=np.uint8).reshape(3, 4, 5) % 9
+    first = FakeLattice((3, 4, 5), seed=1)
+    C.save_state(tmp_path, first, 10, 1.0, {}, labels)
+
+    class Killed(FakeLattice):
+        def macro_all(self, ic=0):
+            raise RuntimeError("job killed")
+
+    with pytest.raises(RuntimeError):
+        C.save_state(tmp_path, Killed((3, 4, 5), seed=2), 20, 1.0, {}, labels)
+    dst = FakeLattice((3, 4, 5), seed=3)
+    cfg = C.load_state(tmp_path, dst, labels)
+    assert cfg["iterations"] == 10 and np.array_equal(dst.df, first.df)
+    # killed between the two renames of the swap: the previous state is under .old
+    (tmp_path / "current_state").rename(tmp_path / "current_state.old")
+    cfg = C.load_state(tmp_path, dst, labels)
+    assert cfg["iterations"] == 10
+    # the next complete save takes over and clears the leftovers
+    second = FakeLattice((3, 4, 5), seed=4)
+    C.save_state(tmp_path, second, 30, 1.0, {}, labels)
+    assert not (tmp_path / "current_state.old").exists() and not (tmp_path / "current_state.tmp").exists()
+    cfg = C.load_state(tmp_path, dst, labels)
+    assert cfg["iterations"] == 30 and np.array_equal(dst.df, second.df)

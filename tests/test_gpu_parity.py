@@ -359,3 +359,50 @@ def test_async_steps_and_control_rows_match_sync():
     b.sync()
     assert np.array_equal(a.export_df(), b.export_df())
     assert np.array_equal(a.stats()[0], b.stats()[0])
+
+
+@pytest.mark.parametrize("dtype,tol_u", [("f32", 5e-5), ("f16", 2e-3), ("bf16", 2e-2)])
+def test_reduced_precision_kbc_n4_cy_local_neq(dtype, tol_u):
+    """KBC_N4 with the local Carreau-Yasuda viscosity, the collision of the storage-precision
+    study, in FP32 / FP16 / BF16 storage against the FP64 oracle after 200 steps, relative to
+    the peak velocity."""
+    orc, lat = _tcpc_pair(O.COLLISIONS.index("KBC_N4"), dtype=dtype, cy_mode=O.CY_LOCAL_NEQ, cy=CY)
+    orc.step(200)
+    lat.step(200, macro=True)
+    fluid = orc.get_map() == G.MAP_FLUID
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
+    for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
+        assert err <= tol_u, (dtype, err)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_watchdog_reports_density_out_of_range_and_recovers(dtype):
+    """The device watchdog (density outside (0.25, 4) or not finite) turns into
+    NNLBM_ERR_NAN with its message; importing a sound state clears it and the case steps on.
+    The bad state is made on the host: nothing on the device faults."""
+    orc, lat = _tcpc_pair(0, dtype=dtype)
+    orc.step(3)
+    good = orc.get_df()
+    labels = orc.get_map()
+    bad = good.copy()
+    z, y, x = [int(v[len(v) // 2]) for v in np.nonzero(labels == G.MAP_FLUID)]
+    bad[:, z, y, x] *= 5.0  # density 5 at one fluid cell
+    lat.import_df(bad)
+    with pytest.raises(capi.NnlbmError) as e:
+        lat.step(1)
+    assert e.value.code == capi.ERR_NAN
+    assert "density" in str(e.value)
+    # asynchronous steps report it at the next sync
+    lat.import_df(bad)
+    lat.step(1, wait=False)
+    with pytest.raises(capi.NnlbmError) as e:
+        lat.sync()
+    assert e.value.code == capi.ERR_NAN
+    # a sound state clears the flag; the case then matches the oracle again
+    lat.import_df(good)
+    lat.step(5)
+    orc.step(5)
+    tol = FP64_TOL if dtype == "f64" else 1e-5
+    fluid = labels == G.MAP_FLUID
+    assert max_rel(lat.export_df()[:, fluid], orc.get_df()[:, fluid]) <= tol

@@ -55,13 +55,15 @@ def test_golden_tcpc_setup():
 
 
 @pytest.mark.parametrize("name", ["step_tcpc_cum", "step_tcpc_kbc_n4", "step_tcpc_kbc_c4", "step_tcpc_bgk_force",
-                                  "step_pipe_mrt", "step_box_cum"])
+                                  "step_tcpc_cum_reffd", "step_tcpc_bgk_reffd", "step_pipe_mrt", "step_box_cum"])
 def test_golden_lattice_steps(name):
     g = _load(name + ".npz")
     col, eq, nu, steps, fx, fy, fz = g["meta"]
+    cy_mode, *cy = g["cy"]
     labels = g["labels"]
     nz, ny, nx = labels.shape
-    orc = O.Oracle(nx, ny, nz, collision=int(col), equilibrium=int(eq), nu=float(nu), force=(fx, fy, fz))
+    orc = O.Oracle(nx, ny, nz, collision=int(col), equilibrium=int(eq), nu=float(nu), force=(fx, fy, fz),
+                   cy_mode=int(cy_mode), cy=tuple(cy))
     orc.set_map(labels)
     orc.set_inflow(*g["inflow"])
     if g["profile"].size:
@@ -71,10 +73,18 @@ def test_golden_lattice_steps(name):
     df = orc.get_df()
     rel = np.abs(df - g["df"]) / np.abs(g["df"])
     assert rel.max() <= 1e-13, rel.max()
-    # reference-driver macro order: rho vx vy vz fx fy fz | vm+x vm-x vmy vmz vmxx vmyy vmzz
-    for fo, fr in ((O.M_RHO, 0), (O.M_VX, 1), (O.M_VY, 2), (O.M_VZ, 3), (O.M_FX, 4), (O.M_VM_PLUS_X, 7),
-                   (O.M_VM_MINUS_X, 8), (O.M_VM_XX, 11), (O.M_VM_ZZ, 13)):
-        np.testing.assert_allclose(orc.get_macro(fo), g["macro"][fr], rtol=0, atol=1e-14)
+    # macro fields in the oracle's numbering: rho, u, the mean/rms sums and the force (the
+    # finite-difference Carreau-Yasuda force of the reffd cases); the strain of the cells
+    # whose strain the step reads (FLUID)
+    for fo in (O.M_RHO, O.M_VX, O.M_VY, O.M_VZ, O.M_VM_PLUS_X, O.M_VM_MINUS_X, O.M_VM_XX, O.M_VM_ZZ, O.M_FX, O.M_FY,
+               O.M_FZ):
+        np.testing.assert_allclose(orc.get_macro(fo), g["macro"][fo], rtol=0, atol=1e-14)
+    fluid = labels == O.FLUID
+    for fo in (O.M_S11, O.M_S12, O.M_S13, O.M_S22, O.M_S32, O.M_S33):
+        np.testing.assert_allclose(orc.get_macro(fo)[fluid], g["macro"][fo][fluid], rtol=0, atol=1e-14)
+    if int(cy_mode) == O.CY_REF_FD:
+        # the coupling was live: the strain force is far from zero
+        assert np.max(np.abs(g["macro"][O.M_FX] - fx)) > 1e-4
 
 
 @pytest.mark.parametrize("col", range(11), ids=O.COLLISIONS)

@@ -13,6 +13,10 @@ This file is named to be collected last; it also passes on its own.
 """
 from __future__ import annotations
 
+import subprocess
+import sys
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -92,7 +96,7 @@ def test_noalloc_refuses_what_it_would_have_to_allocate():
 
 
 def test_noalloc_refuses_more_nodes_than_the_scratch_holds():
-    # 520 x 520 prescribed-velocity inlet nodes: 270,400 x 4 FP32 values > 4 MiB - 256 B
+    # 520 x 520 prescribed-velocity inlet nodes: 270,400 x 4 FP32 values > 4 MiB - 1 KiB
     m, prof = G.dense_box_map(4, 520, 520)
     lat = Lattice(CaseSpec((4, 520, 520), dtype="f32", collision="BGK", nu=0.05))
     lat.set_map(m)
@@ -103,3 +107,54 @@ def test_noalloc_refuses_more_nodes_than_the_scratch_holds():
     msg = capi.last_error(lat.h)
     assert rc == capi.ERR_ARG and "NNLBM_NOALLOC_SCRATCH_BYTES" in msg, msg
     lat.close()
+
+
+# Run in a fresh interpreter (torch switches CUDA's lazy module loading on, as a host
+# application usually has it): free device memory around two no-allocation calls.  First
+# after nnlbm_step has run the kernels once (the documented order), then, printed for the
+# record, in a context whose kernels have never been launched.
+_FRESH = r"""
+import sys
+sys.path[:0] = [sys.argv[1], sys.argv[1] + "/tests"]
+import torch
+from nonnewlbm_b200 import CaseSpec, Lattice, capi
+from helpers import small_junction
+
+def context(collision):
+    wall = small_junction()
+    lat = Lattice(CaseSpec(wall.shape[::-1], dtype="f32", collision=collision, nu=0.02))
+    c = lat.setup_tcpc(wall)
+    lat.set_inflow(ivc_flux=0.03 * c["left_area"], svc_flux=0.02 * c["right_area"])
+    lat.init_equilibrium()
+    return lat
+
+def free():
+    torch.cuda.synchronize(0)
+    return torch.cuda.mem_get_info(0)[0]
+
+def two_calls(lat):
+    for _ in range(2):
+        rc = capi.lib().nnlbm_step_noalloc(lat.h, 5, capi.STEP_REDUCE)
+        assert rc == capi.OK, capi.last_error(lat.h)
+
+free()
+a = context("CUM")
+a.step(1, reduce=True)
+f0 = free()
+two_calls(a)
+f1 = free()
+b = context("BGK")  # a launch group whose kernels this process has not run
+b.step_info(0)
+g0 = free()
+two_calls(b)
+g1 = free()
+print("after-step", f0, f1, "never-launched", g0, g1)
+sys.exit(0 if f1 == f0 else 1)
+"""
+
+
+def test_noalloc_first_calls_take_no_device_memory():
+    """The first two calls in a fresh process leave the device's free memory unchanged."""
+    root = Path(__file__).resolve().parents[1]
+    p = subprocess.run([sys.executable, "-c", _FRESH, str(root)], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout + p.stderr
