@@ -15,7 +15,9 @@ with CUDA events on the library's stream.
 On one GPU the FP32 line also carries, unless --no-extras, the same workload in FP16
 storage with the errors of FP32 and FP16 against FP64 on a short noisy-inflow run
 ("storage_f16"), and, for the junction, the 15-case study batched in one launch group
-against the cases stepped one after another ("batch").
+against the cases stepped one after another ("batch") and the throughput configuration,
+the dense 768x576x480 box, for the cumulant in FP32/FP16/BF16 storage with and without
+the FP64 mean/rms sums, and BGK, MRT_LES and KBC_N4 in FP32 ("dense_box").
 
 Multi-GPU (launched by torchrun, one rank per GPU): every rank runs its own replica of the
 case (the path has no exchange step on one GPU); value = all fluid-cell updates / max time.
@@ -55,7 +57,9 @@ def parse():
     ap.add_argument("--no-stats", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=400)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--no-extras", action="store_true", help="skip the FP16-storage and 15-case batch measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP16-storage, dense-box and 15-case batch measurements")
+    ap.add_argument("--dense-warmup", type=int, default=200)
+    ap.add_argument("--dense-steps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -368,6 +372,64 @@ def storage_comparison(a, flush: L2Flush, dev: int, f32_mlups: float) -> dict:
                          f"seed {err['seed']}"}
 
 
+# the throughput configuration's variants: (collision, storage, FP64 mean/rms on)
+DENSE_VARIANTS = [("CUM", "f32", True), ("CUM", "f32", False), ("CUM", "f16", False), ("CUM", "bf16", False),
+                  ("CUM", "f16", True), ("BGK", "f32", False), ("MRT_LES", "f32", False), ("KBC_N4", "f32", False)]
+
+
+def dense_box_lines(dev: int, warmup: int, steps: int, shape=(768, 576, 480), variants=DENSE_VARIANTS) -> dict:
+    """The dense periodic box (212 M cells, 22.9 GB of FP32 populations, far above L2) for
+    each variant: `warmup` untimed steps, then `steps` steps timed as one block with CUDA
+    events on the library's stream (steady state), the step kernel's mean launch time from
+    events around 5 single launches, its roofline against the measured copy bandwidth, and
+    the clocks sampled during the timed block."""
+    import torch
+
+    from nonnewlbm_b200 import workloads as W
+
+    peak, peak_kind = measured_peaks()
+    out = {"shape": list(shape), "warmup": warmup, "steps": steps,
+           "timing": "one block of steps between two CUDA events (inputs 12-23 GB, far above L2)"}
+    for col, dt, stats in variants:
+        w = W.dense_box(dtype=dt, collision=col, shape=shape)
+        lat = W.build_lattice(w, device=dev)
+        fluid = lat.step_info()["fluid_cells"]
+        lat.autotune(stats=stats)
+        lat.step(warmup, stats=stats)
+        stream = torch.cuda.ExternalStream(lat.stream, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(dev)
+        sampler.start()
+        time.sleep(0.3)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        lat.step(steps, stats=stats, wait=False)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        lat.sync()
+        clocks = sampler.stop()
+        ms = e0.elapsed_time(e1)
+        prof_ms = lat.profile_step(5, stats=stats)
+        k_ms = prof_ms["step"][0]
+        bpu = bytes_per_update(dt, stats)
+        mlups = fluid * steps / (ms / 1e3) / 1e6
+        achieved = fluid * bpu / (k_ms / 1e3) / 1e9
+        key = f"{col}_{dt}_{'stats' if stats else 'nostats'}"
+        out[key] = {"mlups": round(mlups, 1), "ms_per_step": round(ms / steps, 4), "fluid_cells": fluid,
+                    "kernel_ms": round(k_ms, 4),
+                    "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "bytes_per_update": bpu,
+                                 "traffic": ncu_traffic(f"{w.name}:{dt}:{col}:none:{'stats' if stats else 'nostats'}")},
+                    "clocks": clocks}
+        lat.close()
+        del lat
+    for stats in (False, True):
+        s = "stats" if stats else "nostats"
+        if f"CUM_f32_{s}" in out and f"CUM_f16_{s}" in out:
+            out[f"ratio_f16_f32_{s}"] = round(out[f"CUM_f16_{s}"]["mlups"] / out[f"CUM_f32_{s}"]["mlups"], 3)
+    return out
+
+
 def batch_gain(dev: int) -> dict:
     """The 15-case study (5 inflow pairs x 3 rheologies, seeded scales in [0.5, 1]): one
     batched launch group against the cases stepped one after another."""
@@ -462,6 +524,7 @@ def run_ours(a, dist: Dist) -> int:
                 line["storage_f16"] = storage_comparison(a, flush, dev, value)
                 if a.workload == "junction":
                     line["batch"] = batch_gain(dev)
+                    line["dense_box"] = dense_box_lines(dev, a.dense_warmup, a.dense_steps)
         line["reduce_last"] = [float(v) for v in red] if red is not None else None
         print(json.dumps(line))
     return 0

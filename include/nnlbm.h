@@ -205,6 +205,21 @@ int nnlbm_get_macro(nnlbm_ctx* ctx, int ic, int field, double* out);
  * rho*ux split by sign (sim_tcpc.cu:347-348) and only ever uses their sum (:724-725). */
 int nnlbm_get_stats(nnlbm_ctx* ctx, int ic, double* out, int64_t* n_accumulated);
 
+/* The VTK output fields of StateTcpc::outputData (sim_tcpc.cu:684-784), computed on the
+ * device from the macro fields of the last step that had NNLBM_STEP_MACRO and the mean/rms
+ * sums, in double, and stored as float (the type of the file's arrays).  Replaces the
+ * per-cell outputData calls of State::writeVTK_3D_singlefile (state.hpp:782-851).
+ * params[10] = {dx [m], dt [s], density [kg/m^3], lattice reference viscosity
+ *               (dt/dx^2 * nu_inf), Carreau-Yasuda flag (0/1), lattice nu0, lattice lambda,
+ *               a, n, steps summed in the mean/rms sums (at least 1 is used)}.
+ * wall_flags: [nz][ny][nx] wall flags after the planes were opened (LBM::getWall, as returned
+ * by nnlbm_tcpc_labels), read by the near-wall test of wss_proxy_pa; NULL = no walls.
+ * out: [20][nz][ny][nx] floats in file order: velocity (3), mean_velocity (3), lbm_rho,
+ * pressure_pa, gamma_dot, nu_phys_m2_s, mu_phys_pa_s, wss_proxy_pa, turbulence_intensity,
+ * rms_velocity, strain_diag_1_s (3), strain_shear_1_s (3).  Allocates a device buffer of
+ * 20 floats per cell for the call. */
+int nnlbm_output_fields(nnlbm_ctx* ctx, int ic, const double* params, const uint8_t* wall_flags, float* out);
+
 /* Canonical populations (see the layout note above).  Replaces: LBM::copyDFsToHost
  * (core.h:1584) and the df dumps of State::saveState (state.hpp:1552-1721). */
 int nnlbm_export_df(nnlbm_ctx* ctx, int ic, double* out);

@@ -29,8 +29,12 @@ EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
     "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_step_noalloc", "nnlbm_stat_reset", "nnlbm_get_macro",
     "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_import_stats", "nnlbm_import_macro", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_set_launch", "nnlbm_step_info", "nnlbm_profile_step",
-    "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels", "nnlbm_sync",
+    "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels", "nnlbm_sync", "nnlbm_output_fields",
 ]
+# the VTK output fields of nnlbm_output_fields, in file order, with their components
+OUTPUT_FIELDS = [("velocity", 3), ("mean_velocity", 3), ("lbm_rho", 1), ("pressure_pa", 1), ("gamma_dot", 1),
+                 ("nu_phys_m2_s", 1), ("mu_phys_pa_s", 1), ("wss_proxy_pa", 1), ("turbulence_intensity", 1),
+                 ("rms_velocity", 1), ("strain_diag_1_s", 3), ("strain_shear_1_s", 3)]
 
 
 class CaseDesc(ctypes.Structure):
@@ -92,6 +96,7 @@ def lib():
         L.nnlbm_last_error.argtypes = [_vp, ctypes.c_char_p, ctypes.c_size_t]
         L.nnlbm_destroy.argtypes = [_vp]
         L.nnlbm_tcpc_labels.argtypes = [ctypes.c_int32] * 3 + [_vp, _vp, _vp, _vp]
+        L.nnlbm_output_fields.argtypes = [_vp, i, _dp, _vp, _vp]
         _lib = L
     return _lib
 

@@ -95,6 +95,13 @@ void NNLBM_CAT(launch_init_macro_, NNLBM_DT)(const void* args, double rho, doubl
     k_init_macro<NNLBM_DT><<<148 * 8, 256, 0, s>>>(*(const CaseArgs<CT>*)args, (CT)rho, (CT)ux, (CT)uy, (CT)uz);
 }
 
+void NNLBM_CAT(launch_output_fields_, NNLBM_DT)(const void* args, const OutputParams& p, const uint8_t* wall, float* out,
+                                              cudaStream_t s)
+{
+    using CT = typename Storage<NNLBM_DT>::CT;
+    k_output_fields<CT><<<148 * 8, 256, 0, s>>>(*(const CaseArgs<CT>*)args, p, wall, out);
+}
+
 // every kernel of this translation unit resolved now (see load_step in nnlbm_kernels.cuh)
 cudaError_t NNLBM_CAT(load_bc_, NNLBM_DT)()
 {
@@ -103,7 +110,8 @@ cudaError_t NNLBM_CAT(load_bc_, NNLBM_DT)()
                          (const void*)k_bc_gather<NNLBM_DT, false, ARGS_PARAM>, (const void*)k_bc_gather<NNLBM_DT, true, ARGS_PARAM>,
                          (const void*)k_bc_gather<NNLBM_DT, false, ARGS_GLOBAL>, (const void*)k_bc_gather<NNLBM_DT, true, ARGS_GLOBAL>,
                          (const void*)k_refd_velocity<NNLBM_DT, false>, (const void*)k_refd_velocity<NNLBM_DT, true>,
-                         (const void*)k_refd_stress<CT>, (const void*)k_fill_eq<NNLBM_DT>, (const void*)k_init_macro<NNLBM_DT>};
+                         (const void*)k_refd_stress<CT>, (const void*)k_fill_eq<NNLBM_DT>, (const void*)k_init_macro<NNLBM_DT>,
+                         (const void*)k_output_fields<CT>};
     cudaFuncAttributes fa;
     for (const void* f : fns) {
         const cudaError_t e = cudaFuncGetAttributes(&fa, f);

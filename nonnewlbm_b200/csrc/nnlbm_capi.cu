@@ -32,6 +32,7 @@ NNLBM_DECL_STEP_DT(0) NNLBM_DECL_STEP_DT(1) NNLBM_DECL_STEP_DT(2) NNLBM_DECL_STE
     void launch_refd_stress_##DT(bool, dim3, dim3, cudaStream_t, const void*);           \
     void launch_fill_eq_##DT(const void*, double, double, double, double, cudaStream_t); \
     void launch_init_macro_##DT(const void*, double, double, double, double, cudaStream_t); \
+    void launch_output_fields_##DT(const void*, const OutputParams&, const uint8_t*, float*, cudaStream_t); \
     cudaError_t load_bc_##DT();
 NNLBM_DECL_AUX(0) NNLBM_DECL_AUX(1) NNLBM_DECL_AUX(2) NNLBM_DECL_AUX(3)
 
@@ -62,12 +63,13 @@ struct AuxLaunchers {
     GroupLauncher gather, refd_velocity, refd_stress;
     void (*fill_eq)(const void*, double, double, double, double, cudaStream_t);
     void (*init_macro)(const void*, double, double, double, double, cudaStream_t);
+    void (*output_fields)(const void*, const OutputParams&, const uint8_t*, float*, cudaStream_t);
 };
 static const AuxLaunchers& aux_launchers(int dt)
 {
 #define NNLBM_AUXROW(DT)                                                                                   \
     {launch_bc_gather_##DT, launch_refd_velocity_##DT, launch_refd_stress_##DT, launch_fill_eq_##DT,     \
-     launch_init_macro_##DT}
+     launch_init_macro_##DT, launch_output_fields_##DT}
     static const AuxLaunchers t[4] = {NNLBM_AUXROW(0), NNLBM_AUXROW(1), NNLBM_AUXROW(2), NNLBM_AUXROW(3)};
     return t[dt];
 }
@@ -332,6 +334,8 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
             Chunk none = chunks.back();
             none.fluid = 0;
             none.periodic = 0;
+            none.src = 0;
+            none.cflags &= ~CH_SRC;
             chunks.push_back(none);
         }
         for (int32_t k : c.gather_self)
@@ -757,13 +761,35 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 neq += lab == L_IN_EQ;
                 nbc += lab >= L_IN_L;
             }
-    // boundary nodes (open planes and GEO_INFLOW cells), in cell order: each is written by
-    // its own lane of the node warps; the open-plane ones are gathered first
+    // Open-plane nodes whose re-centred stencil is the pull of their inward neighbour (a
+    // FLUID or PERIODIC cell off every face, so that nothing wraps or is clamped) are finished
+    // by that neighbour within the step (serve_nodes in nnlbm_kernels.cuh).  Not with the
+    // finite-difference Carreau-Yasuda force, which the neighbour adds to its own velocity.
     std::vector<uint8_t> dl(map, map + c.N);
+    std::vector<uint8_t> serves((size_t)c.N, 0);
+    const bool can_fuse = c.d.cy_mode != NNLBM_CY_REF_FD;
+    auto fused_source = [&](size_t i, int lab) -> int64_t {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        const int sx = x + (lab == L_IN_L) - (lab == L_IN_R || lab == L_OUT_REQ);
+        const int sy = y + (lab == L_OUT_F) - (lab == L_OUT_B);
+        if (sx < 1 || sx > nx - 2 || sy < 1 || sy > ny - 2 || z < 1 || z > nz - 2) return -1;
+        const size_t s = id(sx, sy, z);
+        return map[s] == L_FLUID || map[s] == L_PERIODIC ? (int64_t)s : -1;
+    };
+    // the other boundary nodes (open planes and GEO_INFLOW cells), in cell order: each is
+    // written by its own lane of the node warps; the open-plane ones are gathered first
     std::vector<int32_t> self_cell, gather_self;
     for (size_t i = 0; i < (size_t)c.N; ++i) {
         const int lab = map[i];
         if (lab != L_IN_EQ && !is_pull_bc(lab)) continue;
+        if (can_fuse && lab != L_IN_EQ) {
+            const int64_t s = fused_source(i, lab);
+            if (s >= 0) {
+                dl[i] |= LF_FUSED;
+                serves[(size_t)s] = 1;
+                continue;
+            }
+        }
         dl[i] |= LF_SELF;
         if (lab != L_IN_EQ) gather_self.push_back((int32_t)self_cell.size());
         self_cell.push_back((int32_t)i);
@@ -790,6 +816,7 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                     if (collides(i)) {
                         ch.fluid |= bit;
                         if (map[i] == L_PERIODIC) ch.periodic |= bit;
+                        if (serves[i]) ch.src |= bit;
                     }
                 }
                 // flags: the chunk lies on a y or z face; the chunk is plain (no colliding cell
@@ -797,7 +824,7 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 const bool face = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
                 const unsigned xface = (x0 == 0 ? 1u : 0u) | (nx - 1 - x0 < kChunk ? 1u << (nx - 1 - x0) : 0u);
                 const bool plain = !face && !(ch.fluid & xface);
-                ch.cflags = CH_FLUID | (face ? CH_FACE : 0) | (plain ? CH_PLAIN : 0);
+                ch.cflags = CH_FLUID | (face ? CH_FACE : 0) | (plain ? CH_PLAIN : 0) | (ch.src ? CH_SRC : 0);
                 chunks.push_back(ch);
             }
     c.label.assign(map, map + c.N);
@@ -1156,6 +1183,44 @@ int nnlbm_reduce(nnlbm_ctx* ctx, int ic, double* out5)
         for (int i = 0; i < kRedStripes; ++i) v += r[8 * i + k];
         out5[k] = v;
     }
+    return NNLBM_OK;
+}
+
+int nnlbm_output_fields(nnlbm_ctx* ctx, int ic, const double* params, const uint8_t* wall_flags, float* out)
+{
+    int rc = check_case(ctx, ic);
+    if (rc) return rc;
+    if (!params || !out) return set_err(ctx, NNLBM_ERR_ARG, "null parameters or output");
+    Case& c = ctx->cases[ic];
+    const OutputParams p = {params[0], params[1], params[2], params[3], params[4], params[5],
+                            params[6], params[7], params[8], std::max(1.0, params[9])};
+    if (!(p.dx > 0 && p.dt > 0) || (p.cy != 0.0 && !(p.a > 0)))
+        return set_err(ctx, NNLBM_ERR_ARG, "output fields need dx > 0, dt > 0 and, with Carreau-Yasuda, a > 0");
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = ensure_macro(ctx, c)) != NNLBM_OK) return rc;
+    const size_t N = (size_t)c.N;
+    uint8_t* d_wall = nullptr;
+    float* d_out = nullptr;
+    CK(cudaMalloc(&d_wall, N));
+    const cudaError_t e = cudaMalloc(&d_out, (size_t)kOutputValues * N * sizeof(float));
+    if (e != cudaSuccess) {
+        cudaFree(d_wall);
+        return set_err(ctx, NNLBM_ERR_OOM, "output buffer of %zu bytes: %s", (size_t)kOutputValues * N * sizeof(float),
+                       cudaGetErrorString(e));
+    }
+    // the field values of the last step that stored them, after every step still queued
+    cudaError_t err = wall_flags ? cudaMemcpyAsync(d_wall, wall_flags, N, cudaMemcpyHostToDevice, ctx->stream)
+                                 : cudaMemsetAsync(d_wall, 0, N, ctx->stream);
+    if (err == cudaSuccess) {
+        aux_launchers(c.d.dtype).output_fields(c.args.data(), p, d_wall, d_out, ctx->stream);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(out, d_out, (size_t)kOutputValues * N * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_wall);
+    cudaFree(d_out);
+    if (err != cudaSuccess) return set_err(ctx, NNLBM_ERR_CUDA, "output fields: %s", cudaGetErrorString(err));
     return NNLBM_OK;
 }
 

@@ -41,9 +41,9 @@ namespace nnlbm {
 
 enum : int { L_FLUID = 0, L_WALL = 1, L_PERIODIC = 2, L_IN_L = 3, L_IN_R = 4, L_OUT_F = 5, L_OUT_B = 6,
              L_IN_EQ = 7, L_OUT_REQ = 8 };
-// flag bit of the device label byte (the low four bits hold the label): a boundary node
-// of the node list
-enum : int { LF_SELF = 0x40, L_MASK = 0x0f };
+// flag bits of the device label byte (the low four bits hold the label): a boundary node
+// of the node list; an open-plane node finished by its inward neighbour (serve_nodes)
+enum : int { LF_SELF = 0x40, LF_FUSED = 0x20, L_MASK = 0x0f };
 enum : int { CY_NONE = 0, CY_REF_FD = 1, CY_LOCAL_NEQ = 2 };
 enum : int { F_STATS = 1, F_MACRO = 2, F_REDUCE = 4 };
 // macro field order of the context's macro array
@@ -119,15 +119,17 @@ struct CaseArgs {
 };
 
 // one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
-// and per lane (bit = lane) which cells collide and which of those are PERIODIC
+// and per lane (bit = lane) which cells collide, which of those are PERIODIC and which
+// finish open-plane nodes next to them (serve_nodes)
 struct alignas(16) Chunk {
-    int c0, yz, cflags, pad0;
+    int c0, yz, cflags;
+    unsigned src;
     unsigned fluid, periodic, pad1, pad2;
 };
 // chunk flags (bits 16.. of cflags, the case index below).  CH_PLAIN: no neighbour of any
 // colliding lane wraps around the box (the chunk is off the y/z faces and has no
-// colliding cell at x = 0 or nx-1)
-enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PLAIN = 1 << 18 };
+// colliding cell at x = 0 or nx-1); CH_SRC: some lane finishes an open-plane node
+enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PLAIN = 1 << 18, CH_SRC = 1 << 19 };
 
 // a launch group: cases sharing storage type and collision.  Up to kParamCases cases also
 // travel in the kernel parameters (read through the constant cache, indexed by the
@@ -275,6 +277,50 @@ __device__ __forceinline__ double node_outputs(const CaseArgs<CT>& a, int flags,
     return lab == L_IN_L ? (double)ux : lab == L_IN_R ? -(double)ux : lab == L_OUT_F ? -(double)uy : lab == L_OUT_B ? (double)uy : 0.0;
 }
 
+// Open-plane nodes finished by their inward neighbour.  A node's re-centred stencil
+// (sim_tcpc.cu:242-273, lbm_bc.h:147-152) pulls the populations of the step around the cell
+// one plane inward; where that cell collides and none of its neighbours wraps or is
+// clamped, this is exactly the pull of that cell itself, and in the A-A layout every slot
+// the stencil reads is read and overwritten by that cell alone within the step.  So the
+// cell's own pre-collision density and velocity are the node's gathered values: the cell
+// writes the node's equilibrium into the node's slots (which no other cell touches within
+// the step) and the node's outputs, and no separate gather, with its wait before the first
+// store, is needed.  The host marks such nodes LF_FUSED and their cells in the chunk's src
+// mask.  (x, y, z) is the serving cell; it may serve one node along x and one along y.
+template <int DT, bool ODD>
+__device__ __noinline__ void serve_nodes(const CaseArgs<typename Storage<DT>::CT>* ap, int c, int x, int y, int z,
+                                         typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
+                                         typename Storage<DT>::CT uy, typename Storage<DT>::CT uz, int step, int flags)
+{
+    using CT = typename Storage<DT>::CT;
+    const CaseArgs<CT>& a = *ap;
+    const int sy = a.nx;
+    const int nb[4] = {c - 1, c + 1, c - sy, c + sy};
+    for (int d = 0; d < 4; ++d) {
+        const int lb = a.label[nb[d]];
+        if (!(lb & LF_FUSED)) continue;
+        const int lab = lb & L_MASK;
+        const bool mine = d == 0 ? lab == L_IN_L : d == 1 ? (lab == L_IN_R || lab == L_OUT_REQ) : d == 2 ? lab == L_OUT_F
+                                                                                                         : lab == L_OUT_B;
+        if (!mine) continue;
+        CT r = CT(1), u = ux, v = uy, w = uz;
+        if (lab == L_IN_L || lab == L_IN_R) { // rho one cell inward, plug velocity (sim_tcpc.cu:242-261)
+            const StepCtl<CT>& ctl = a.ctl[step];
+            r = rho;
+            u = lab == L_IN_L ? ctl.u_left : ctl.u_right;
+            v = CT(0);
+            w = CT(0);
+        }
+        const int n = nb[d];
+        store_node_eq<DT, ODD>(a, n, x - (d == 0) + (d == 1), y - (d == 2) + (d == 3), z, r, u, v, w);
+        const double qn = node_outputs<CT>(a, flags, lab, n, r, u, v, w);
+        if ((flags & F_REDUCE) && qn != 0.0) {
+            const int slot = lab == L_IN_L ? 1 : lab == L_IN_R ? 2 : lab == L_OUT_F ? 3 : lab == L_OUT_B ? 4 : 0;
+            if (slot) atomicAdd(red_stripe(a.red, n) + slot, qn);
+        }
+    }
+}
+
 // the finite-difference Carreau-Yasuda force of CY_REF_FD (core.h:663-781), kept out of
 // line so that it takes no registers from the bulk path:
 // divergence of the strain of the previous phase with one-sided differences next to
@@ -413,6 +459,10 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         if (flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
         if (!(rho > CT(0.25) && rho < CT(4))) atomicOr(a.err, 1);
         mass = (double)rho;
+        if (ch.src & bit) {
+            const int y = ch.yz & 0xffff, z = ch.yz >> 16;
+            serve_nodes<DT, ODD>(ap, c, ch.c0 - y * a.nx - z * a.nx * a.ny + lane, y, z, rho, ux, uy, uz, step, flags);
+        }
     }
     if (flags & F_REDUCE) {
         const double s0 = warp_sum(mass);
@@ -445,8 +495,8 @@ template <> struct Cook<3> {
 // the rest of a pair once its populations f (raw stored value + weight, or the rest state
 // where the cell does not collide) are in registers: collision, stores, per-cell outputs
 template <int DT, int COL, bool ODD>
-__device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, f2* f, int step,
-                                            int flags, int lane)
+__device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const CaseArgs<float>* ap, const Chunk& ca,
+                                            const Chunk& cb, f2* f, int step, int flags, int lane)
 {
     using T = typename Storage<DT>::T;
     const unsigned bit = 1u << lane;
@@ -487,6 +537,12 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Chun
             if (flags & F_STATS) accumulate_stats<float>(a, cc[h], r[h], u0[h], u1[h], u2[h]);
             if (!(r[h] > 0.25f && r[h] < 4.f)) atomicOr(a.err, 1);
             mass += (double)r[h];
+            const Chunk& ch = h ? cb : ca;
+            if (ch.src & bit) {
+                const int y = ch.yz & 0xffff, z = ch.yz >> 16;
+                serve_nodes<DT, ODD>(ap, cc[h], ch.c0 - y * a.nx - z * a.nx * a.ny + lane, y, z, r[h], u0[h], u1[h], u2[h],
+                                     step, flags);
+            }
         }
     }
     if (flags & F_REDUCE) {
@@ -583,7 +639,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
             if (pairable<ARGS>(g, ca, cb)) {
                 f2 f[27];
                 pair_load<DT, ODD>(a, ca, cb, lane, f);
-                pair_finish<DT, COL, ODD>(a, ca, cb, f, step, flags, lane);
+                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, f, step, flags, lane);
             } else {
                 fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, step, flags, lane);
                 if (cb.fluid) {
@@ -748,6 +804,64 @@ __global__ void __launch_bounds__(256) k_refd_stress(const __grid_constant__ Gro
 }
 
 // ---------------------------------------------------------------------------------------
+// VTK output fields (StateTcpc::outputData, sim_tcpc.cu:684-784), per cell in double like the
+// reference's host code and stored as float, the type of the file's arrays
+// ---------------------------------------------------------------------------------------
+// physical scales of one output call (sim_tcpc.cu:716-745): lattice -> physical velocity,
+// the physical density, the lattice reference viscosity and the Carreau-Yasuda law
+struct OutputParams {
+    double dx, dt, density, nu_lbm;
+    double cy, nu0, lambda, a, n;  // cy != 0: Carreau-Yasuda material
+    double diff;                   // steps summed in the mean/rms sums, at least 1
+};
+// fields in file order, 20 values a cell: velocity (3), mean_velocity (3), lbm_rho,
+// pressure_pa, gamma_dot, nu_phys_m2_s, mu_phys_pa_s, wss_proxy_pa, turbulence_intensity,
+// rms_velocity, strain_diag_1_s (3), strain_shear_1_s (3)
+constexpr int kOutputValues = 20;
+
+template <class CT>
+__global__ void __launch_bounds__(256) k_output_fields(const CaseArgs<CT> a, const OutputParams p, const uint8_t* wall,
+                                                       float* out)
+{
+    const int64_t N = a.N;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < N; c += (int64_t)gridDim.x * blockDim.x) {
+        const CT* M = a.macro;
+        const double v2p = p.dx / p.dt;
+        const double vx = (double)M[M_VX * N + c] * v2p, vy = (double)M[M_VY * N + c] * v2p, vz = (double)M[M_VZ * N + c] * v2p;
+        double s[6] = {0, 0, 0, 0, 0, 0};
+        if (a.stats) {
+            for (int k = 0; k < 6; ++k)
+                s[k] = a.stats_f64 ? ((const double*)a.stats)[k * N + c] : (double)((const float*)a.stats)[k * N + c];
+        }
+        const double mx = s[0] * v2p / p.diff, my = s[1] * v2p / p.diff, mz = s[2] * v2p / p.diff;
+        const double rx = fabs(s[3] * v2p * v2p / p.diff - mx * mx), ry = fabs(s[4] * v2p * v2p / p.diff - my * my);
+        const double rz = fabs(s[5] * v2p * v2p / p.diff - mz * mz);
+        const double rms = sqrt(rx * rx + ry * ry + rz * rz);
+        const double meanv = sqrt(mx * mx + my * my + mz * mz);
+        const double turb = fabs(meanv) <= 1e-10 ? 0.0 : rms / fabs(meanv);
+        const double rho = (double)M[M_RHO * N + c];
+        const double pressure = (rho - 1.0) * p.density * (v2p * v2p / 3.0);
+        const double S11 = M[M_S11 * N + c], S12 = M[M_S12 * N + c], S13 = M[M_S13 * N + c];
+        const double S22 = M[M_S22 * N + c], S32 = M[M_S32 * N + c], S33 = M[M_S33 * N + c];
+        const double gl = sqrt(2.0) * sqrt(S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * (S12 * S12 + S13 * S13 + S32 * S32));
+        const double gdot = gl / p.dt;
+        const double nul = p.cy != 0.0 ? p.nu_lbm + (p.nu0 - p.nu_lbm) * pow(1.0 + pow(gl * p.lambda, p.a), (p.n - 1.0) / p.a)
+                                       : p.nu_lbm;
+        const double nup = nul * p.dx * p.dx / p.dt;
+        const double mup = nup * p.density;
+        // nearWall (sim_tcpc.cu:709-714): a wall among the six neighbours inside the box
+        const int x = (int)(c % a.nx), y = (int)((c / a.nx) % a.ny), z = (int)(c / ((int64_t)a.nx * a.ny));
+        const int64_t sy = a.nx, sz = (int64_t)a.nx * a.ny;
+        const bool near = (x > 0 && wall[c - 1]) || (x < a.nx - 1 && wall[c + 1]) || (y > 0 && wall[c - sy]) ||
+                          (y < a.ny - 1 && wall[c + sy]) || (z > 0 && wall[c - sz]) || (z < a.nz - 1 && wall[c + sz]);
+        const double v[kOutputValues] = {vx, vy, vz, mx, my, mz, rho, pressure, gdot, nup, mup, near ? mup * gdot : 0.0,
+                                         turb, rms, S11 / p.dt, S22 / p.dt, S33 / p.dt, S12 / p.dt, S13 / p.dt, S32 / p.dt};
+#pragma unroll
+        for (int k = 0; k < kOutputValues; ++k) out[k * N + c] = (float)v[k];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // host-side dispatch: one function per (storage, collision) instantiated in its own
 // translation unit
 // ---------------------------------------------------------------------------------------
@@ -821,7 +935,9 @@ cudaError_t load_step_variant()
 {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_step<DT, COL, ODD, ARGS, false>);
-    if (e == cudaSuccess && pairs_chunks(DT, COL)) e = cudaFuncGetAttributes(&fa, (const void*)k_step<DT, COL, ODD, ARGS, true>);
+    if constexpr (pairs_chunks(DT, COL)) {
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void*)k_step<DT, COL, ODD, ARGS, true>);
+    }
     return e;
 }
 template <int DT, int COL>

@@ -184,6 +184,28 @@ class Lattice:
             raise ValueError("macro array size does not match the lattice")
         self._chk(capi.lib().nnlbm_import_macro(self.h, ic, capi.dptr(a)))
 
+    def output_fields(self, dx: float, dt: float, density: float, nu_lbm: float, cy=None, steps_summed: int = 1,
+                      wall_flags: np.ndarray | None = None, ic: int = 0) -> list:
+        """The VTK output fields of case ic computed on the device (nnlbm_output_fields), as
+        [(name, float32 array [z][y][x] or [3][z][y][x])] in file order.  cy: the lattice
+        Carreau-Yasuda parameters (nu0, lambda, a, n) of a Carreau-Yasuda material, else None."""
+        n = self.ncells(ic)
+        p = np.array([dx, dt, density, nu_lbm, 0.0 if cy is None else 1.0, *(cy if cy is not None else (0, 0, 1, 1)),
+                      float(steps_summed)], dtype=np.float64)
+        out = np.empty(20 * n, dtype=np.float32)
+        wf = None if wall_flags is None else np.ascontiguousarray(wall_flags, dtype=np.uint8).reshape(-1)
+        if wf is not None and wf.size != n:
+            raise ValueError("wall flags must have one byte per cell")
+        self._chk(capi.lib().nnlbm_output_fields(self.h, ic, capi.dptr(p), None if wf is None else wf.ctypes.data,
+                                                 out.ctypes.data))
+        shape = self.shape(ic)
+        fields, k = [], 0
+        for name, dofs in capi.OUTPUT_FIELDS:
+            a = out[k * n:(k + dofs) * n].reshape((dofs,) + shape) if dofs > 1 else out[k * n:(k + 1) * n].reshape(shape)
+            fields.append((name, a))
+            k += dofs
+        return fields
+
     def reduce(self, ic: int = 0) -> np.ndarray:
         out = np.zeros(5)
         self._chk(capi.lib().nnlbm_reduce(self.h, ic, capi.dptr(out)))

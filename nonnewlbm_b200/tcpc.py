@@ -20,7 +20,6 @@ the state and stop when reached) and --savestate-period SECONDS (wall-clock peri
 """
 from __future__ import annotations
 
-import math
 import os
 import sys
 import time
@@ -167,46 +166,12 @@ class TcpcRun:
 
     # -- outputs (sim_tcpc.cu:684-784) ---------------------------------------------------
     def output_fields(self):
-        L, dx, dt, mat = self.lat, self.dx, self.dt, self.mat
-        v2p = dx / dt
-        u = np.stack([L.macro(capi.M_VX), L.macro(capi.M_VY), L.macro(capi.M_VZ)]) * v2p
-        st, _ = L.stats()
-        diff = max(1.0, float(self.iterations - self.prev_iter))
-        mean = st[:3] * v2p / diff
-        meansq = st[3:] * v2p * v2p / diff
-        rms_c = np.abs(meansq - mean * mean)
-        rms = np.sqrt((rms_c ** 2).sum(axis=0))
-        meanv = np.sqrt((mean ** 2).sum(axis=0))
-        turb = np.where(np.abs(meanv) <= 1e-10, 0.0, rms / np.where(meanv == 0, 1.0, np.abs(meanv)))
-        rho = L.macro(capi.M_RHO)
-        cs2_phys = (dx / dt) ** 2 / 3.0
-        pressure = (rho - 1.0) * mat.density * cs2_phys
-        S = np.stack([L.macro(f) for f in (capi.M_S11, capi.M_S12, capi.M_S13, capi.M_S22, capi.M_S32, capi.M_S33)])
-        S11, S12, S13, S22, S32, S33 = S
-        gamma_lbm = math.sqrt(2.0) * np.sqrt(S11 ** 2 + S22 ** 2 + S33 ** 2 + 2.0 * (S12 ** 2 + S13 ** 2 + S32 ** 2))
-        gamma_dot = gamma_lbm / dt
-        nu_lbm_ref = dt / dx / dx * mat.nu_inf
-        if mat.carreau_yasuda:
-            c = self.conv
-            nu_lbm = nu_lbm_ref + (c["nu0"] - nu_lbm_ref) * np.power(1.0 + np.power(gamma_lbm * c["lambda"], c["a"]),
-                                                                     (c["n"] - 1.0) / c["a"])
-        else:
-            nu_lbm = np.full(rho.shape, nu_lbm_ref)
-        nu_phys = nu_lbm * dx * dx / dt
-        mu_phys = nu_phys * mat.density
-        wf = self.wall_flags
-        near = np.zeros(wf.shape, dtype=bool)
-        near[:, :, 1:] |= wf[:, :, :-1]
-        near[:, :, :-1] |= wf[:, :, 1:]
-        near[:, 1:, :] |= wf[:, :-1, :]
-        near[:, :-1, :] |= wf[:, 1:, :]
-        near[1:, :, :] |= wf[:-1, :, :]
-        near[:-1, :, :] |= wf[1:, :, :]
-        wss = np.where(near, mu_phys * gamma_dot, 0.0)
-        return [("velocity", u), ("mean_velocity", mean), ("lbm_rho", rho), ("pressure_pa", pressure),
-                ("gamma_dot", gamma_dot), ("nu_phys_m2_s", nu_phys), ("mu_phys_pa_s", mu_phys), ("wss_proxy_pa", wss),
-                ("turbulence_intensity", turb), ("rms_velocity", rms),
-                ("strain_diag_1_s", np.stack([S11, S22, S33]) / dt), ("strain_shear_1_s", np.stack([S12, S13, S32]) / dt)]
+        """The fields of StateTcpc::outputData (sim_tcpc.cu:716-784), computed on the device."""
+        mat, c = self.mat, self.conv
+        nu_lbm_ref = self.dt / self.dx / self.dx * mat.nu_inf
+        cy = (c["nu0"], c["lambda"], c["a"], c["n"]) if mat.carreau_yasuda else None
+        return self.lat.output_fields(self.dx, self.dt, mat.density, nu_lbm_ref, cy=cy,
+                                      steps_summed=max(1, self.iterations - self.prev_iter), wall_flags=self.wall_flags)
 
     def write_vtk(self, count: int) -> Path:
         d = self.dir / "vtk3D"
