@@ -17,7 +17,7 @@ storage with the errors of FP32 and FP16 against FP64 on a short noisy-inflow ru
 ("storage_f16"), and, for the junction, the 15-case study batched in one launch group
 against the cases stepped one after another ("batch") and the throughput configuration,
 the dense 768x576x480 box, for the cumulant in FP32/FP16/BF16 storage with and without
-the FP64 mean/rms sums, and BGK, MRT_LES and KBC_N4 in FP32 ("dense_box").
+the FP64 mean/rms sums, BGK and MRT_LES in FP32 and FP16, and KBC_N4 in FP32 ("dense_box").
 
 Multi-GPU (launched by torchrun, one rank per GPU): every rank runs its own replica of the
 case (the path has no exchange step on one GPU); value = all fluid-cell updates / max time.
@@ -374,7 +374,8 @@ def storage_comparison(a, flush: L2Flush, dev: int, f32_mlups: float) -> dict:
 
 # the throughput configuration's variants: (collision, storage, FP64 mean/rms on)
 DENSE_VARIANTS = [("CUM", "f32", True), ("CUM", "f32", False), ("CUM", "f16", False), ("CUM", "bf16", False),
-                  ("CUM", "f16", True), ("BGK", "f32", False), ("MRT_LES", "f32", False), ("KBC_N4", "f32", False)]
+                  ("CUM", "f16", True), ("BGK", "f32", False), ("BGK", "f16", False), ("MRT_LES", "f32", False),
+                  ("MRT_LES", "f16", False), ("KBC_N4", "f32", False)]
 
 
 def dense_box_lines(dev: int, warmup: int, steps: int, shape=(768, 576, 480), variants=DENSE_VARIANTS) -> dict:
@@ -423,10 +424,13 @@ def dense_box_lines(dev: int, warmup: int, steps: int, shape=(768, 576, 480), va
                     "clocks": clocks}
         lat.close()
         del lat
-    for stats in (False, True):
-        s = "stats" if stats else "nostats"
-        if f"CUM_f32_{s}" in out and f"CUM_f16_{s}" in out:
-            out[f"ratio_f16_f32_{s}"] = round(out[f"CUM_f16_{s}"]["mlups"] / out[f"CUM_f32_{s}"]["mlups"], 3)
+    # FP16 over FP32 storage, per collision and accumulator setting
+    for col in sorted({v[0] for v in variants}):
+        for stats in (False, True):
+            s = "stats" if stats else "nostats"
+            a16, a32 = out.get(f"{col}_f16_{s}"), out.get(f"{col}_f32_{s}")
+            if a16 and a32:
+                out[f"ratio_f16_f32_{col}_{s}"] = round(a16["mlups"] / a32["mlups"], 3)
     return out
 
 
