@@ -107,7 +107,19 @@ typedef struct {
     double cy_nu0, cy_lambda, cy_a, cy_n; /* Carreau-Yasuda, lattice units */
     double fx, fy, fz;   /* homogeneous body force */
     double storage_scale; /* multiplier of the shifted populations f-w in F16/BF16 storage; 0 = default */
+    int32_t bounce_back; /* NNLBM_BB_* */
+    int32_t reserved;    /* 0 */
 } nnlbm_case_desc;
+
+/* wall treatment (nnlbm_case_desc.bounce_back) */
+enum {
+    NNLBM_BB_FULLWAY = 0, /* wall nodes: a wall cell returns the reversed populations it pulled, two steps
+                             after they left (the reference's only wall, lbm_streaming.h:78-107) */
+    NNLBM_BB_HALFWAY = 1  /* link-wise: a population that would come from a wall cell is the cell's own
+                             post-collision population of the opposite direction of the previous
+                             step, one step after it left; applies to every pull, the re-centred
+                             stencils of the open planes included.  No reference counterpart. */
+};
 
 typedef struct nnlbm_ctx nnlbm_ctx;
 

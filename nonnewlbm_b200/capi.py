@@ -46,6 +46,8 @@ class CaseDesc(ctypes.Structure):
         ("cy_a", ctypes.c_double), ("cy_n", ctypes.c_double),
         ("fx", ctypes.c_double), ("fy", ctypes.c_double), ("fz", ctypes.c_double),
         ("storage_scale", ctypes.c_double),
+        ("bounce_back", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

@@ -11,7 +11,9 @@
 
 namespace nnlbm {
 
-// every slot q of every cell <- feq_q(rho, u): a uniform state is valid in either A-A layout
+// every slot q of every cell <- feq_q(rho, u): a uniform state is valid in either A-A layout.
+// With halfway bounce-back the layout an odd step leaves (the one written here) keeps a
+// non-wall cell's population opp(q) in its own slot q where x - c_q is a wall.
 template <int DT>
 __global__ void k_fill_eq(const CaseArgs<typename Storage<DT>::CT> a, typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
                           typename Storage<DT>::CT uy, typename Storage<DT>::CT uz)
@@ -21,8 +23,9 @@ __global__ void k_fill_eq(const CaseArgs<typename Storage<DT>::CT> a, typename S
     CT f[27];
     equilibrium<CT>(a.eq, rho, ux, uy, uz, f);
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.N; c += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t m = (a.hw && (a.label[c] & L_MASK) != L_WALL) ? a.hw[c] : 0u;
 #pragma unroll
-        for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, q), (int)c, q, f[q], a.scale);
+        for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, q), (int)c, q, ((m >> oppq(q)) & 1u) ? f[oppq(q)] : f[q], a.scale);
     }
 }
 

@@ -81,6 +81,8 @@ namespace {
 
 const int kStorageBytes[4] = {8, 4, 2, 2};
 const int kChunk = 32;
+// which open-plane node a cell finishes (per cell while the work list is built)
+enum : uint8_t { kServeXneg = 1, kServeXpos = 2, kServeXreq = 4, kServeYneg = 8, kServeYpos = 16 };
 // slack around the populations and after the labels: every kernel reads only cells of the
 // box, so nothing is read here; the slack keeps each allocation's start and end away from
 // the first and last 32-cell row
@@ -115,6 +117,8 @@ struct Case {
     int64_t ctl_cap = 0;
     double* d_red = nullptr;         // in the context's status block
     int* d_err = nullptr;            // in the context's status block
+    uint32_t* d_hw = nullptr;        // halfway bounce-back: wall-neighbour bits per cell
+    std::vector<uint32_t> hw;        // its host copy (empty with full-way bounce-back)
     // host state
     std::vector<uint8_t> label;      // plain solver labels
     std::vector<uint8_t> dlabel;     // labels with the work flags of the device copy
@@ -220,6 +224,7 @@ void fill_case_args(const Case& c, CaseArgs<CT>& a)
     a.ctl = (const StepCtl<CT>*)c.d_ctl;
     a.red = c.d_red;
     a.err = c.d_err;
+    a.hw = c.d_hw;
     // slot bases (integer arithmetic: a shifted base may point before the array; the cell
     // index of every plain access brings it back inside)
     const uintptr_t base = (uintptr_t)c.df;
@@ -334,7 +339,7 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
             Chunk none = chunks.back();
             none.fluid = 0;
             none.periodic = 0;
-            none.src = 0;
+            none.xneg = none.xpos = none.xreq = none.yneg = none.ypos = 0;
             none.cflags &= ~CH_SRC;
             chunks.push_back(none);
         }
@@ -560,6 +565,11 @@ size_t canon_index(const Case& c, int x, int y, int z, int q, int* slot)
         *slot = oppq(q);
         return (size_t)x + (size_t)nx * (y + (size_t)ny * z);
     }
+    const size_t self = (size_t)x + (size_t)nx * (y + (size_t)ny * z);
+    if (!c.hw.empty() && ((c.hw[self] >> q) & 1u)) { // halfway bounce-back towards a wall: own slot opp(q)
+        *slot = oppq(q);
+        return self;
+    }
     *slot = q; // after an odd step (or the initial state): slot q at x + c_q
     const int xx = (x + cxq(q) + nx) % nx, yy = (y + cyq(q) + ny) % ny, zz = (z + czq(q) + nz) % nz;
     return (size_t)xx + (size_t)nx * (yy + (size_t)ny * zz);
@@ -684,6 +694,8 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
                            "equilibrium 0..3, cy_mode 0..2, nu > 0)", i);
         if (d.cy_mode != NNLBM_CY_NONE && !(d.cy_a > 0 && d.cy_nu0 > 0))
             return set_err(ctx, NNLBM_ERR_ARG, "case %d: Carreau-Yasuda needs a > 0 and nu0 > 0", i);
+        if (d.bounce_back != NNLBM_BB_FULLWAY && d.bounce_back != NNLBM_BB_HALFWAY)
+            return set_err(ctx, NNLBM_ERR_ARG, "case %d: bounce_back must be NNLBM_BB_FULLWAY or NNLBM_BB_HALFWAY", i);
         if (d.ny > 65535 || d.nz > 65535) return set_err(ctx, NNLBM_ERR_ARG, "case %d: ny and nz are limited to 65535", i);
         c.N = (int64_t)d.nx * d.ny * d.nz;
         if (c.N >= (int64_t)1 << 31) return set_err(ctx, NNLBM_ERR_ARG, "case %d: %lld cells exceed 2^31", i, (long long)c.N);
@@ -785,14 +797,29 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
         if (can_fuse && lab != L_IN_EQ) {
             const int64_t s = fused_source(i, lab);
             if (s >= 0) {
-                dl[i] |= LF_FUSED;
-                serves[(size_t)s] = 1;
+                serves[(size_t)s] |= lab == L_IN_L ? kServeXneg : lab == L_IN_R ? kServeXpos
+                                   : lab == L_OUT_REQ ? (kServeXpos | kServeXreq) : lab == L_OUT_F ? kServeYneg : kServeYpos;
                 continue;
             }
         }
         dl[i] |= LF_SELF;
         if (lab != L_IN_EQ) gather_self.push_back((int32_t)self_cell.size());
         self_cell.push_back((int32_t)i);
+    }
+    // halfway bounce-back: per cell, bit q where the neighbour x + c_q (wrapped) is a wall
+    std::vector<uint32_t> hw;
+    if (c.d.bounce_back == NNLBM_BB_HALFWAY) {
+        hw.assign((size_t)c.N, 0u);
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y)
+                for (int x = 0; x < nx; ++x) {
+                    uint32_t m = 0;
+                    for (int q = 0; q < 27; ++q) {
+                        const int xx = (x + cxq(q) + nx) % nx, yy = (y + cyq(q) + ny) % ny, zz = (z + czq(q) + nz) % nz;
+                        if (q != 13 && map[id(xx, yy, zz)] == L_WALL) m |= 1u << q;
+                    }
+                    hw[id(x, y, z)] = m;
+                }
     }
     // packed work list of 32-cell row chunks of colliding cells: a chunk starts at the first
     // colliding cell not yet covered in its row, rounded down to a 32-byte boundary of the
@@ -816,15 +843,21 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                     if (collides(i)) {
                         ch.fluid |= bit;
                         if (map[i] == L_PERIODIC) ch.periodic |= bit;
-                        if (serves[i]) ch.src |= bit;
+                        if (serves[i] & kServeXneg) ch.xneg |= bit;
+                        if (serves[i] & kServeXpos) ch.xpos |= bit;
+                        if (serves[i] & kServeXreq) ch.xreq |= bit;
+                        if (serves[i] & kServeYneg) ch.yneg |= bit;
+                        if (serves[i] & kServeYpos) ch.ypos |= bit;
+                        if (!hw.empty() && hw[i]) ch.cflags |= CH_HW;
                     }
                 }
                 // flags: the chunk lies on a y or z face; the chunk is plain (no colliding cell
                 // on an x face either, so no neighbour index wraps)
                 const bool face = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
                 const unsigned xface = (x0 == 0 ? 1u : 0u) | (nx - 1 - x0 < kChunk ? 1u << (nx - 1 - x0) : 0u);
-                const bool plain = !face && !(ch.fluid & xface);
-                ch.cflags = CH_FLUID | (face ? CH_FACE : 0) | (plain ? CH_PLAIN : 0) | (ch.src ? CH_SRC : 0);
+                const bool plain = !face && !(ch.fluid & xface) && !(ch.cflags & CH_HW);
+                const bool serving = (ch.xneg | ch.xpos | ch.yneg | ch.ypos) != 0;
+                ch.cflags |= CH_FLUID | (face ? CH_FACE : 0) | (plain ? CH_PLAIN : 0) | (serving ? CH_SRC : 0);
                 chunks.push_back(ch);
             }
     c.label.assign(map, map + c.N);
@@ -837,6 +870,11 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->stream)); // no queued step still reads the old labels
     CK(cudaMemcpy(c.d_label, dl.data(), (size_t)c.N, cudaMemcpyHostToDevice));
+    if (!hw.empty()) {
+        if (!c.d_hw) CK(cudaMalloc(&c.d_hw, (size_t)c.N * sizeof(uint32_t)));
+        CK(cudaMemcpy(c.d_hw, hw.data(), (size_t)c.N * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    c.hw = hw;
     c.has_map = true;
     rebuild_case_args(ctx, c);
     return NNLBM_OK;
@@ -1154,6 +1192,9 @@ int nnlbm_import_df(nnlbm_ctx* ctx, int ic, const double* in)
         for (int z = 0; z < nz; ++z)
             for (int y = 0; y < ny; ++y)
                 for (int x = 0; x < nx; ++x) {
+                    // with halfway bounce-back nothing reads a wall cell's populations, and
+                    // the slots the layout would give them hold their neighbours' reflections
+                    if (!c.hw.empty() && c.label[x + (size_t)nx * (y + (size_t)ny * z)] == L_WALL) continue;
                     int slot;
                     const size_t i = canon_index(c, x, y, z, q, &slot);
                     encode(c, raw.data() + (size_t)slot * c.q_stride * eb, i, q,
@@ -1511,7 +1552,7 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
             if (p) cudaFree(p);
     }
     for (Case& c : ctx->cases) {
-        void* ptrs[] = {c.df_base, c.d_label, c.d_macro, c.d_stats, c.d_ctl};
+        void* ptrs[] = {c.df_base, c.d_label, c.d_macro, c.d_stats, c.d_ctl, c.d_hw};
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }

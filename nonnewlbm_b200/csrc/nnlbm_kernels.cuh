@@ -41,9 +41,9 @@ namespace nnlbm {
 
 enum : int { L_FLUID = 0, L_WALL = 1, L_PERIODIC = 2, L_IN_L = 3, L_IN_R = 4, L_OUT_F = 5, L_OUT_B = 6,
              L_IN_EQ = 7, L_OUT_REQ = 8 };
-// flag bits of the device label byte (the low four bits hold the label): a boundary node
-// of the node list; an open-plane node finished by its inward neighbour (serve_nodes)
-enum : int { LF_SELF = 0x40, LF_FUSED = 0x20, L_MASK = 0x0f };
+// flag bit of the device label byte (the low four bits hold the label): a boundary node
+// of the node list
+enum : int { LF_SELF = 0x40, L_MASK = 0x0f };
 enum : int { CY_NONE = 0, CY_REF_FD = 1, CY_LOCAL_NEQ = 2 };
 enum : int { F_STATS = 1, F_MACRO = 2, F_REDUCE = 4 };
 // macro field order of the context's macro array
@@ -108,6 +108,9 @@ struct CaseArgs {
     const StepCtl<CT>* ctl;
     double* red;               // [kRedStripes][8]: stripes of {mass, Q_ivc, Q_svc, Q_out5, Q_out6}
     int* err;                  // watchdog flag
+    // halfway bounce-back only (null otherwise): per cell, bit q set where cell x + c_q is a
+    // WALL cell (neighbours wrap around the box like the A-A stores)
+    const uint32_t* hw;
     // per-slot base addresses of a plain chunk's accesses, each the population array of one
     // slot already offset by the cell shift of the access, so that an address is one
     // shift-and-add of the cell index: slot q (even step, loads of slot q and stores of
@@ -119,17 +122,25 @@ struct CaseArgs {
 };
 
 // one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
-// and per lane (bit = lane) which cells collide, which of those are PERIODIC and which
-// finish open-plane nodes next to them (serve_nodes)
+// and per lane (bit = lane) which cells collide, which of those are PERIODIC, and which
+// finish an open-plane node next to them (serve_nodes): the node at x-1 (IN_L), at x+1
+// (IN_R, or OUT_REQ where the lane is in xreq too), at y-1 (OUT_F), at y+1 (OUT_B)
 struct alignas(16) Chunk {
     int c0, yz, cflags;
-    unsigned src;
-    unsigned fluid, periodic, pad1, pad2;
+    unsigned fluid, periodic;
+    unsigned xneg, xpos, xreq, yneg, ypos;
+    unsigned pad0, pad1;
 };
 // chunk flags (bits 16.. of cflags, the case index below).  CH_PLAIN: no neighbour of any
 // colliding lane wraps around the box (the chunk is off the y/z faces and has no
 // colliding cell at x = 0 or nx-1); CH_SRC: some lane finishes an open-plane node
-enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PLAIN = 1 << 18, CH_SRC = 1 << 19 };
+enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PLAIN = 1 << 18, CH_SRC = 1 << 19,
+             CH_HW = 1 << 20 };
+// CH_HW (halfway bounce-back): some colliding lane has a WALL neighbour; such chunks take the
+// general path, whose odd step reads a population arriving from a wall from the cell's own
+// slot q (where the previous, even, step left its f*_opp(q)) and stores a population leaving
+// towards a wall into its own slot opp(q) (where the next, even, step reads it): each
+// reflects one step after it left
 
 // a launch group: cases sharing storage type and collision.  Up to kParamCases cases also
 // travel in the kernel parameters (read through the constant cache, indexed by the
@@ -282,41 +293,113 @@ __device__ __forceinline__ double node_outputs(const CaseArgs<CT>& a, int flags,
 // one plane inward; where that cell collides and none of its neighbours wraps or is
 // clamped, this is exactly the pull of that cell itself, and in the A-A layout every slot
 // the stencil reads is read and overwritten by that cell alone within the step.  So the
-// cell's own pre-collision density and velocity are the node's gathered values: the cell
-// writes the node's equilibrium into the node's slots (which no other cell touches within
-// the step) and the node's outputs, and no separate gather, with its wait before the first
-// store, is needed.  The host marks such nodes LF_FUSED and their cells in the chunk's src
-// mask.  (x, y, z) is the serving cell; it may serve one node along x and one along y.
+// cell's own pre-collision density and velocity are the node's gathered values: after the
+// chunk's cells have stored, the node's equilibrium goes into the node's slots (which no
+// other cell touches within the step) with the node's outputs, and no separate gather, with
+// its wait before the first store, is needed.  The chunk's lane masks say which nodes its
+// lanes finish.  Where few lanes serve (an inlet row has one), the whole warp writes each
+// node, lane q storing population q; where many serve (an outlet row), each lane writes its
+// own.
+
+// the node of serving lane direction d (0: x-1, 1: x+1, 2: y-1, 3: y+1) and its label
+__device__ __forceinline__ int served_label(int d, bool req)
+{
+    return d == 0 ? L_IN_L : d == 1 ? (req ? L_OUT_REQ : L_IN_R) : d == 2 ? L_OUT_F : L_OUT_B;
+}
+
+// density and velocity of a served node from its inward cell's (sim_tcpc.cu:242-273,
+// lbm_bc.h:147-152): the inflow planes take the cell's density and the plug velocity, the
+// outlets rho = 1 and the cell's velocity
+template <class CT>
+__device__ __forceinline__ void served_state(int lab, CT rho, CT ux, CT uy, CT uz, const StepCtl<CT>& ctl, CT& r, CT& u, CT& v,
+                                             CT& w)
+{
+    if (lab == L_IN_L || lab == L_IN_R) {
+        r = rho; u = lab == L_IN_L ? ctl.u_left : ctl.u_right; v = CT(0); w = CT(0);
+    } else {
+        r = CT(1); u = ux; v = uy; w = uz;
+    }
+}
+
+// element offset, from the slot base of this step's store of population q, of node n at
+// (xn, yn, zn): the cell itself in the even step; x + c_q wrapped around the box in the odd
+// step, from a base already shifted by c_q (slot_odd_st)
+__device__ __forceinline__ int node_wrap(int xn, int yn, int zn, int q, int nx, int ny, int nz)
+{
+    const int x = xn + cxq(q), y = yn + cyq(q), z = zn + czq(q);
+    return (x < 0 ? nx : x >= nx ? -nx : 0) + nx * ((y < 0 ? ny : y >= ny ? -ny : 0) + ny * (z < 0 ? nz : z >= nz ? -nz : 0));
+}
+
+// the node's macro / stats / flux outputs (by one lane)
+template <class CT>
+__device__ __forceinline__ void served_outputs(const CaseArgs<CT>& a, int flags, int lab, int n, CT r, CT u, CT v, CT w)
+{
+    const double qn = node_outputs<CT>(a, flags, lab, n, r, u, v, w);
+    if ((flags & F_REDUCE) && qn != 0.0) {
+        const int slot = lab == L_IN_L ? 1 : lab == L_IN_R ? 2 : lab == L_OUT_F ? 3 : lab == L_OUT_B ? 4 : 0;
+        if (slot) atomicAdd(red_stripe(a.red, n) + slot, qn);
+    }
+}
+
+// called by the whole warp of a chunk with serving lanes (CH_SRC), after its stores; rho and
+// u are each lane's pre-collision values
 template <int DT, bool ODD>
-__device__ __noinline__ void serve_nodes(const CaseArgs<typename Storage<DT>::CT>* ap, int c, int x, int y, int z,
+__device__ __noinline__ void serve_nodes(const CaseArgs<typename Storage<DT>::CT>* ap, const Chunk* chp, int lane,
                                          typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
                                          typename Storage<DT>::CT uy, typename Storage<DT>::CT uz, int step, int flags)
 {
-    using CT = typename Storage<DT>::CT;
+    using S = Storage<DT>;
+    using T = typename S::T;
+    using CT = typename S::CT;
     const CaseArgs<CT>& a = *ap;
-    const int sy = a.nx;
-    const int nb[4] = {c - 1, c + 1, c - sy, c + sy};
-    for (int d = 0; d < 4; ++d) {
-        const int lb = a.label[nb[d]];
-        if (!(lb & LF_FUSED)) continue;
-        const int lab = lb & L_MASK;
-        const bool mine = d == 0 ? lab == L_IN_L : d == 1 ? (lab == L_IN_R || lab == L_OUT_REQ) : d == 2 ? lab == L_OUT_F
-                                                                                                         : lab == L_OUT_B;
-        if (!mine) continue;
-        CT r = CT(1), u = ux, v = uy, w = uz;
-        if (lab == L_IN_L || lab == L_IN_R) { // rho one cell inward, plug velocity (sim_tcpc.cu:242-261)
-            const StepCtl<CT>& ctl = a.ctl[step];
-            r = rho;
-            u = lab == L_IN_L ? ctl.u_left : ctl.u_right;
-            v = CT(0);
-            w = CT(0);
+    // the record is read again here rather than kept in registers through the collision
+    const int c0 = chp->c0, yz = chp->yz;
+    const unsigned xneg = chp->xneg, xpos = chp->xpos, xreq = chp->xreq, yneg = chp->yneg, ypos = chp->ypos;
+    const int y = yz & 0xffff, z = yz >> 16;
+    const int sy = a.nx, x0 = c0 - y * sy - z * sy * a.ny;
+    const StepCtl<CT>& ctl = a.ctl[step];
+    const unsigned masks[4] = {xneg, xpos, yneg, ypos};
+    const unsigned src = xneg | xpos | yneg | ypos;
+    if (__popc(src) > 4) {
+        // many serving lanes: each writes its own nodes
+        const unsigned bit = 1u << lane;
+        for (int d = 0; d < 4; ++d) {
+            if (!(masks[d] & bit)) continue;
+            const int lab = served_label(d, (xreq & bit) != 0);
+            const int xn = x0 + lane - (d == 0) + (d == 1), yn = y - (d == 2) + (d == 3);
+            const int n = c0 + lane + (d == 0 ? -1 : d == 1 ? 1 : d == 2 ? -sy : sy);
+            CT r, u, v, w;
+            served_state<CT>(lab, rho, ux, uy, uz, ctl, r, u, v, w);
+            CT f[27];
+            equilibrium<CT>(a.eq, r, u, v, w, f);
+#pragma unroll
+            for (int q = 0; q < 27; ++q) {
+                if (!ODD) S::store((T*)a.slot_even[oppq(q)], n, q, f[q], a.scale);
+                else S::store((T*)a.slot_odd_st[q], n + node_wrap(xn, yn, z, q, a.nx, a.ny, a.nz), q, f[q], a.scale);
+            }
+            served_outputs<CT>(a, flags, lab, n, r, u, v, w);
         }
-        const int n = nb[d];
-        store_node_eq<DT, ODD>(a, n, x - (d == 0) + (d == 1), y - (d == 2) + (d == 3), z, r, u, v, w);
-        const double qn = node_outputs<CT>(a, flags, lab, n, r, u, v, w);
-        if ((flags & F_REDUCE) && qn != 0.0) {
-            const int slot = lab == L_IN_L ? 1 : lab == L_IN_R ? 2 : lab == L_OUT_F ? 3 : lab == L_OUT_B ? 4 : 0;
-            if (slot) atomicAdd(red_stripe(a.red, n) + slot, qn);
+        return;
+    }
+    // few serving lanes: the warp writes each node, lane q population q
+    for (unsigned todo = src; todo; todo &= todo - 1) {
+        const int s = __ffs(todo) - 1;
+        const CT rs = __shfl_sync(0xffffffffu, rho, s), us = __shfl_sync(0xffffffffu, ux, s);
+        const CT vs = __shfl_sync(0xffffffffu, uy, s), ws = __shfl_sync(0xffffffffu, uz, s);
+        for (int d = 0; d < 4; ++d) {
+            if (!((masks[d] >> s) & 1u)) continue;
+            const int lab = served_label(d, ((xreq >> s) & 1u) != 0);
+            const int xn = x0 + s - (d == 0) + (d == 1), yn = y - (d == 2) + (d == 3);
+            const int n = c0 + s + (d == 0 ? -1 : d == 1 ? 1 : d == 2 ? -sy : sy);
+            CT r, u, v, w;
+            served_state<CT>(lab, rs, us, vs, ws, ctl, r, u, v, w);
+            if (lane < 27) {
+                const int q = lane;
+                const CT fq = feq_one<CT>(a.eq, q, r, u, v, w);
+                if (!ODD) S::store((T*)a.slot_even[oppq(q)], n, q, fq, a.scale);
+                else S::store((T*)a.slot_odd_st[q], n + node_wrap(xn, yn, z, q, a.nx, a.ny, a.nz), q, fq, a.scale);
+            }
+            if (lane == s) served_outputs<CT>(a, flags, lab, n, r, u, v, w);
         }
     }
 }
@@ -389,13 +472,14 @@ struct StepRegs {
 // ---------------------------------------------------------------------------------------
 template <int DT, int COL, bool ODD>
 __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>::CT>& a, const CaseArgs<typename Storage<DT>::CT>* ap,
-                                            const Chunk& ch, int step, int flags, int lane)
+                                            const Chunk& ch, const Chunk* chp, int step, int flags, int lane)
 {
     using S = Storage<DT>;
     using T = typename S::T;
     using CT = typename S::CT;
     double mass = 0.0;
     const unsigned bit = 1u << lane;
+    CT rho = CT(1), ux = CT(0), uy = CT(0), uz = CT(0);
     if (ch.fluid & bit) {
         const int c = ch.c0 + lane;
         const int64_t qs = a.qstride, sy = a.nx, sz = (int64_t)a.nx * a.ny;
@@ -408,6 +492,8 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
                    sz * wrapc(z + sign * czq(q), a.nz) - c;
         };
         const T* pc = (const T*)a.df + c;
+        // halfway bounce-back: which neighbours are walls (CH_HW chunks, odd step only)
+        const uint32_t hwm = (ODD && (ch.cflags & CH_HW)) ? a.hw[c] : 0u;
         CT f[27];
         if (!ODD) {
             // slot q at c
@@ -419,7 +505,8 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
             for (int q = 0; q < 27; ++q) f[q] = S::from(((const T*)a.slot_odd_ld[q])[c], q, a.inv_scale);
         } else {
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = S::from(pc[oppq(q) * qs + nbr(q, -1)], q, a.inv_scale);
+            for (int q = 0; q < 27; ++q)
+                f[q] = S::from(((hwm >> oppq(q)) & 1u) ? pc[q * qs] : pc[oppq(q) * qs + nbr(q, -1)], q, a.inv_scale);
         }
         CT fx = a.fx, fy = a.fy, fz = a.fz;
         if (a.cy_mode == CY_REF_FD && !(ch.periodic & bit)) {
@@ -427,7 +514,6 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
             refd_force<CT>(ap, c, (int)sy, (int)sz, F);
             fx = F[0]; fy = F[1]; fz = F[2];
         }
-        CT rho, ux, uy, uz;
         density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
         // one inlined collision for both viscosity models (the local Carreau-Yasuda law is
         // a runtime branch inside it)
@@ -447,7 +533,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
             for (int q = 0; q < 27; ++q) S::store((T*)a.slot_odd_st[q], c, q, f[q], a.scale);
         } else {
 #pragma unroll
-            for (int q = 0; q < 27; ++q) S::store(ps, q * qs + nbr(q, 1), q, f[q], a.scale);
+            for (int q = 0; q < 27; ++q) S::store(ps, ((hwm >> q) & 1u) ? oppq(q) * qs : q * qs + nbr(q, 1), q, f[q], a.scale);
         }
         if ((flags & F_MACRO) || a.cy_mode == CY_REF_FD) {
             write_macro<CT>(a, c, rho, ux, uy, uz, fx, fy, fz);
@@ -459,11 +545,8 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         if (flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
         if (!(rho > CT(0.25) && rho < CT(4))) atomicOr(a.err, 1);
         mass = (double)rho;
-        if (ch.src & bit) {
-            const int y = ch.yz & 0xffff, z = ch.yz >> 16;
-            serve_nodes<DT, ODD>(ap, c, ch.c0 - y * a.nx - z * a.nx * a.ny + lane, y, z, rho, ux, uy, uz, step, flags);
-        }
     }
+    if (ch.cflags & CH_SRC) serve_nodes<DT, ODD>(ap, chp, lane, rho, ux, uy, uz, step, flags);
     if (flags & F_REDUCE) {
         const double s0 = warp_sum(mass);
         if (lane == 0 && s0 != 0.0) atomicAdd(red_stripe(a.red, global_warp()), s0);
@@ -496,12 +579,13 @@ template <> struct Cook<3> {
 // where the cell does not collide) are in registers: collision, stores, per-cell outputs
 template <int DT, int COL, bool ODD>
 __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const CaseArgs<float>* ap, const Chunk& ca,
-                                            const Chunk& cb, f2* f, int step, int flags, int lane)
+                                            const Chunk& cb, const Chunk* cap, f2* f, int step, int flags, int lane)
 {
     using T = typename Storage<DT>::T;
     const unsigned bit = 1u << lane;
     const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
     double mass = 0.0;
+    float r[2] = {1.f, 1.f}, u0[2] = {0.f, 0.f}, u1[2] = {0.f, 0.f}, u2[2] = {0.f, 0.f};
     if (fa || fb) {
         const int cA = ca.c0 + lane, cB = cb.c0 + lane;
         const f2 fx(a.fx), fy(a.fy), fz(a.fz);
@@ -521,7 +605,8 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Case
             if (fa) p[cA] = Cook<DT>::put(v.v.x);
             if (fb) p[cB] = Cook<DT>::put(v.v.y);
         }
-        const float r[2] = {rho.v.x, rho.v.y}, u0[2] = {ux.v.x, ux.v.y}, u1[2] = {uy.v.x, uy.v.y}, u2[2] = {uz.v.x, uz.v.y};
+        r[0] = rho.v.x; r[1] = rho.v.y; u0[0] = ux.v.x; u0[1] = ux.v.y;
+        u1[0] = uy.v.x; u1[1] = uy.v.y; u2[0] = uz.v.x; u2[1] = uz.v.y;
         const bool on[2] = {fa, fb};
         const int cc[2] = {cA, cB};
 #pragma unroll
@@ -537,13 +622,11 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Case
             if (flags & F_STATS) accumulate_stats<float>(a, cc[h], r[h], u0[h], u1[h], u2[h]);
             if (!(r[h] > 0.25f && r[h] < 4.f)) atomicOr(a.err, 1);
             mass += (double)r[h];
-            const Chunk& ch = h ? cb : ca;
-            if (ch.src & bit) {
-                const int y = ch.yz & 0xffff, z = ch.yz >> 16;
-                serve_nodes<DT, ODD>(ap, cc[h], ch.c0 - y * a.nx - z * a.nx * a.ny + lane, y, z, r[h], u0[h], u1[h], u2[h],
-                                     step, flags);
-            }
         }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        if ((h ? cb : ca).cflags & CH_SRC) serve_nodes<DT, ODD>(ap, cap + h, lane, r[h], u0[h], u1[h], u2[h], step, flags);
     }
     if (flags & F_REDUCE) {
         const double s0 = warp_sum(mass);
@@ -639,12 +722,12 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
             if (pairable<ARGS>(g, ca, cb)) {
                 f2 f[27];
                 pair_load<DT, ODD>(a, ca, cb, lane, f);
-                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, f, step, flags, lane);
+                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, g.chunks + 2 * w, f, step, flags, lane);
             } else {
-                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, step, flags, lane);
+                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, g.chunks + 2 * w, step, flags, lane);
                 if (cb.fluid) {
                     const int cj = cb.cflags & CH_CASE_MASK;
-                    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, step, flags, lane);
+                    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, g.chunks + 2 * w + 1, step, flags, lane);
                 }
             }
         } else {
@@ -654,7 +737,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
         if (w < g.n_chunks) {
             const Chunk ch = g.chunks[w];
             const int ci = ch.cflags & CH_CASE_MASK;
-            fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, ci), g.cases + ci, ch, step, flags, lane);
+            fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, ci), g.cases + ci, ch, g.chunks + w, step, flags, lane);
         } else {
             node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
         }
@@ -666,26 +749,42 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
 // ---------------------------------------------------------------------------------------
 // canonical post-collision population q of cell (x,y,z) of the previous step, in the A-A
 // layout that step left behind
+__device__ __forceinline__ int clamp_cell(int nx, int ny, int nz, int x, int y, int z)
+{
+    return min(max(x, 0), nx - 1) + nx * (min(max(y, 0), ny - 1) + ny * min(max(z, 0), nz - 1));
+}
+
 template <int DT, bool ODD>
 __device__ __forceinline__ typename Storage<DT>::CT canon(const CaseArgs<typename Storage<DT>::CT>& a, int x, int y, int z, int q)
 {
     using S = Storage<DT>;
     x = min(max(x, 0), a.nx - 1); y = min(max(y, 0), a.ny - 1); z = min(max(z, 0), a.nz - 1);
     const int sy = a.nx, sz = a.nx * a.ny;
+    const int c = x + sy * y + sz * z;
     if (ODD) // the previous (even) step stored f*_q of x in slot opp(q) at x
-        return S::load(qptr<DT>(a, oppq(q)), x + sy * y + sz * z, q, a.inv_scale);
-    // the previous (odd) step, or the initial state, stored f*_q of x in slot q at x + c_q
+        return S::load(qptr<DT>(a, oppq(q)), c, q, a.inv_scale);
+    // the previous (odd) step, or the initial state, stored f*_q of x in slot q at x + c_q, or,
+    // with halfway bounce-back towards a wall, in slot opp(q) at x
+    if (a.hw && ((a.hw[c] >> q) & 1u)) return S::load(qptr<DT>(a, oppq(q)), c, q, a.inv_scale);
     return S::load(qptr<DT>(a, q), wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz), q,
                    a.inv_scale);
 }
 
-// LBM_STREAMING::streaming with explicit (m, centre, p) triples (lbm_streaming.h:10-39)
+// LBM_STREAMING::streaming with explicit (m, centre, p) triples (lbm_streaming.h:10-39); with
+// halfway bounce-back a population that would come from a WALL cell is the centre's own
+// post-collision population of the opposite direction
 template <int DT, bool ODD>
 __device__ __forceinline__ void pull_triples(const CaseArgs<typename Storage<DT>::CT>& a, const int* xs, const int* ys, const int* zs,
                                              typename Storage<DT>::CT* f)
 {
 #pragma unroll
-    for (int q = 0; q < 27; ++q) f[q] = canon<DT, ODD>(a, xs[1 - cxq(q)], ys[1 - cyq(q)], zs[1 - czq(q)], q);
+    for (int q = 0; q < 27; ++q) {
+        const int sx = xs[1 - cxq(q)], sy = ys[1 - cyq(q)], sz = zs[1 - czq(q)];
+        if (a.hw && (a.label[clamp_cell(a.nx, a.ny, a.nz, sx, sy, sz)] & L_MASK) == L_WALL)
+            f[q] = canon<DT, ODD>(a, xs[1], ys[1], zs[1], oppq(q));
+        else
+            f[q] = canon<DT, ODD>(a, sx, sy, sz, q);
+    }
 }
 
 template <int DT, bool ODD, int ARGS>

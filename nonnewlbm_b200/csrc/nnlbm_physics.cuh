@@ -106,53 +106,47 @@ __device__ __forceinline__ CT inv_cum_factor(int c, CT v)
     return c == 0 ? CT(3) * v * v - CT(2) : (c > 0 ? CT(3) * v * v + CT(3) * v + CT(1) : CT(3) * v * v - CT(3) * v + CT(1));
 }
 
-// feq of kind `eq` (runtime-uniform switch) into f[27]
+// population q of the equilibrium of kind `eq` (q and eq may be runtime values; equilibrium()
+// below evaluates the same expression for every q)
 template <class CT>
-__device__ void equilibrium(int eq, CT rho, CT ux, CT uy, CT uz, CT* f)
+__device__ __forceinline__ CT feq_one(int eq, int q, CT rho, CT ux, CT uy, CT uz)
 {
+    const int cx = cxq(q), cy = cyq(q), cz = czq(q);
     if (eq == EQ_DEFAULT) {
         // LBM_EQ_DEFAULT, lbm_eq.h:12-47
         const CT u2 = ux * ux + uy * uy + uz * uz;
-#pragma unroll
-        for (int q = 0; q < 27; ++q) {
-            const CT cu = CT(cxq(q)) * ux + CT(cyq(q)) * uy + CT(czq(q)) * uz;
-            f[q] = weight<CT>(q) * rho * (CT(1) - CT(1.5) * u2 + CT(3) * cu + CT(4.5) * cu * cu);
-        }
-    } else if (eq == EQ_ENTROPIC) {
+        const CT cu = CT(cx) * ux + CT(cy) * uy + CT(cz) * uz;
+        return weight<CT>(q) * rho * (CT(1) - CT(1.5) * u2 + CT(3) * cu + CT(4.5) * cu * cu);
+    }
+    if (eq == EQ_ENTROPIC) {
         // LBM_EQ_ENTROPIC, lbm_eq_entropic.h:12-38: per axis weight (2/3 or 1/6) times
         // (2 - sqrt(1+3v^2)) times B^c with B = (2v + sqrt(1+3v^2)) / (1 - v)
         const CT sx = dsqrt<CT>(CT(1) + CT(3) * ux * ux), sy = dsqrt<CT>(CT(1) + CT(3) * uy * uy);
         const CT sz = dsqrt<CT>(CT(1) + CT(3) * uz * uz);
         const CT bx = (CT(2) * ux + sx) / (CT(1) - ux), by = (CT(2) * uy + sy) / (CT(1) - uy), bz = (CT(2) * uz + sz) / (CT(1) - uz);
         const CT base = (CT(2) - sx) * (CT(2) - sy) * (CT(2) - sz);
-#pragma unroll
-        for (int q = 0; q < 27; ++q) {
-            CT v = (cxq(q) ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) * (cyq(q) ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) *
-                   (czq(q) ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) * base;
-            if (cxq(q) > 0) v *= bx; else if (cxq(q) < 0) v *= CT(1) / bx;
-            if (cyq(q) > 0) v *= by; else if (cyq(q) < 0) v *= CT(1) / by;
-            if (czq(q) > 0) v *= bz; else if (czq(q) < 0) v *= CT(1) / bz;
-            f[q] = rho * v;
-        }
-    } else {
-        // factorised equilibrium of LBM_EQ_INV_CUM (lbm_eq_inv_cum.h:71-101): prefactor by
-        // the number of zero components 3: -1/27, 2: 1/54, 1: -1/108, 0: 1/216
-        CT X[3], Y[3], Z[3];
-#pragma unroll
-        for (int c = -1; c <= 1; ++c) {
-            X[c + 1] = inv_cum_factor<CT>(c, ux);
-            Y[c + 1] = inv_cum_factor<CT>(c, uy);
-            Z[c + 1] = inv_cum_factor<CT>(c, uz);
-        }
-#pragma unroll
-        for (int q = 0; q < 27; ++q) {
-            const int nz0 = nnzq(q);
-            const CT pre = nz0 == 0 ? CT(-1.0 / 27.0) : nz0 == 1 ? CT(1.0 / 54.0) : nz0 == 2 ? CT(-1.0 / 108.0) : CT(1.0 / 216.0);
-            f[q] = pre * rho * (X[cxq(q) + 1] * Y[cyq(q) + 1] * Z[czq(q) + 1]);
-        }
-        // the shipped feq_pmm multiplies by rho twice (lbm_eq_inv_cum.h:49)
-        if (eq == EQ_INV_CUM_REF) f[18] *= rho;
+        CT v = (cx ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) * (cy ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) * (cz ? CT(1.0 / 6.0) : CT(2.0 / 3.0)) * base;
+        if (cx > 0) v *= bx; else if (cx < 0) v *= CT(1) / bx;
+        if (cy > 0) v *= by; else if (cy < 0) v *= CT(1) / by;
+        if (cz > 0) v *= bz; else if (cz < 0) v *= CT(1) / bz;
+        return rho * v;
     }
+    // factorised equilibrium of LBM_EQ_INV_CUM (lbm_eq_inv_cum.h:71-101): prefactor by the
+    // number of zero components 3: -1/27, 2: 1/54, 1: -1/108, 0: 1/216
+    const int nz0 = nnzq(q);
+    const CT pre = nz0 == 0 ? CT(-1.0 / 27.0) : nz0 == 1 ? CT(1.0 / 54.0) : nz0 == 2 ? CT(-1.0 / 108.0) : CT(1.0 / 216.0);
+    CT v = pre * rho * (inv_cum_factor<CT>(cx, ux) * inv_cum_factor<CT>(cy, uy) * inv_cum_factor<CT>(cz, uz));
+    // the shipped feq_pmm multiplies by rho twice (lbm_eq_inv_cum.h:49)
+    if (eq == EQ_INV_CUM_REF && q == 18) v *= rho;
+    return v;
+}
+
+// feq of kind `eq` (runtime-uniform switch) into f[27]
+template <class CT>
+__device__ __forceinline__ void equilibrium(int eq, CT rho, CT ux, CT uy, CT uz, CT* f)
+{
+#pragma unroll
+    for (int q = 0; q < 27; ++q) f[q] = feq_one<CT>(eq, q, rho, ux, uy, uz);
 }
 
 // ---------------------------------------------------------------------------------------

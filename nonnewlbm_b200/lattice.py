@@ -27,6 +27,7 @@ class CaseSpec:
     force: tuple = (0.0, 0.0, 0.0)
     stats_f64: bool = True
     storage_scale: float = 0.0
+    bounce_back: str = "fullway"       # fullway (wall nodes, the reference) | halfway
 
     def desc(self) -> capi.CaseDesc:
         nx, ny, nz = self.shape
@@ -37,7 +38,8 @@ class CaseSpec:
                              capi.EQUILIBRIA[self.equilibrium.lower()], capi.CY_MODES[self.cy_mode.lower()],
                              int(bool(self.stats_f64)), float(self.nu), float(self.cy[0]), float(self.cy[1]),
                              float(self.cy[2]), float(self.cy[3]), float(self.force[0]), float(self.force[1]),
-                             float(self.force[2]), float(self.storage_scale))
+                             float(self.force[2]), float(self.storage_scale),
+                             {"fullway": 0, "halfway": 1}[self.bounce_back.lower()], 0)
 
 
 class Lattice:

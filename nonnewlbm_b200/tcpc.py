@@ -12,7 +12,8 @@ boundary setup flags ``terminate``).  The step itself runs in libnnlbm.so.
 
 Extra options of this build: --dtype (f32 default, f16, bf16, f64), --collision (CUM
 default; KBC_N1..N4, KBC_C1..C4, MRT_LES, BGK), --cy-mode (none = the single-rank reference,
-ref-fd, local-neq), --equilibrium, --device, --results-root, --ramp-steps, and the state
+ref-fd, local-neq), --equilibrium, --bounce-back (fullway default, the reference's wall
+nodes; halfway), --device, --results-root, --ramp-steps, and the state
 checkpoint knobs the reference keeps in State (state.h:229-257): --wall-time SECONDS (save
 the state and stop when reached) and --savestate-period SECONDS (wall-clock period of the
 `savestate` flag check).  A `results_<id>/loadstate` flag resumes from the saved state
@@ -60,6 +61,7 @@ class TcpcOptions:
     collision: str = "CUM"
     cy_mode: str = "none"
     equilibrium: str = "inv_cum_ref"
+    bounce_back: str = "fullway"    # fullway (wall nodes, the reference) | halfway
     device: int = 0
     results_root: str = "."
     ramp_steps: int = 0
@@ -75,7 +77,7 @@ def parse_args(argv) -> TcpcOptions:
            "--lbm-viscosity": "lbm_viscosity", "--wall-time": "wall_time", "--savestate-period": "savestate_period"}
     text = {"--geometry": "geometry", "--material": "material", "--case-id": "case_id", "--output-id": "case_id",
             "--dtype": "dtype", "--collision": "collision", "--cy-mode": "cy_mode", "--equilibrium": "equilibrium",
-            "--results-root": "results_root"}
+            "--results-root": "results_root", "--bounce-back": "bounce_back"}
     ints = {"--block-size": "block_size", "--device": "device", "--ramp-steps": "ramp_steps"}
     i = 0
     while i < len(argv):
@@ -132,7 +134,8 @@ class TcpcRun:
         self.terminate = rc == capi.ERR_AREA
         cy = (conv["nu0"], conv["lambda"], conv["a"], conv["n"])
         self.lat = Lattice(CaseSpec((nx, ny, nz), collision=o.collision, dtype=o.dtype, equilibrium=o.equilibrium,
-                                    cy_mode=o.cy_mode if mat.carreau_yasuda else "none", nu=conv["nu"], cy=cy),
+                                    cy_mode=o.cy_mode if mat.carreau_yasuda else "none", nu=conv["nu"], cy=cy,
+                                    bounce_back=o.bounce_back),
                            device=o.device)
         self.lat.set_map(self.map)
         self.ivc = units.flux_lbm(o.ivc_mls, dx, self.dt)

@@ -683,12 +683,19 @@ static void neighbours(const orc_lattice* L, int x, int y, int z, int lab, int x
 }
 
 /* LBM_STREAMING::streaming (lbm_streaming.h:10-39): f_q <- src at x - c_q, taken from the
- * supplied (xm,x,xp) triples; a triple may be re-centred on a neighbour by the BCs */
+ * supplied (xm,x,xp) triples; a triple may be re-centred on a neighbour by the BCs.
+ * With halfway bounce-back (no reference counterpart: the reference has wall nodes only,
+ * lbm_streaming.h:78-107) a population that would come from a WALL cell is the centre's own
+ * post-collision population of the opposite direction, f_q <- src_opp(q) at the centre; the
+ * rule holds for every pull, the re-centred stencils of the open planes included. */
 static void pull(const orc_lattice* L, const double* src, const int xs[3], const int ys[3],
                  const int zs[3], double* f)
 {
-    for (int q = 0; q < NQ; ++q)
-        f[q] = src[cidx(L, xs[1 - CXq(q)], ys[1 - CYq(q)], zs[1 - CZq(q)]) * NQ + q];
+    const int64_t centre = cidx(L, xs[1], ys[1], zs[1]);
+    for (int q = 0; q < NQ; ++q) {
+        const int64_t s = cidx(L, xs[1 - CXq(q)], ys[1 - CYq(q)], zs[1 - CZq(q)]);
+        f[q] = (L->d.halfway_bounce_back && L->map[s] == ORC_WALL) ? src[centre * NQ + OPP(q)] : src[s * NQ + q];
+    }
 }
 
 /* streamingBounceBack (lbm_streaming.h:78-107): f_{opp q} <- incoming f_q */
@@ -828,14 +835,7 @@ static void cell_step(orc_lattice* L, const double* src, double* dst, int x, int
     }
 
     if (lab == ORC_FLUID || lab == ORC_PERIODIC) {
-        if (d->halfway_bounce_back) {
-            for (int q = 0; q < NQ; ++q) {
-                int64_t s = cidx(L, xs[1 - CXq(q)], ys[1 - CYq(q)], zs[1 - CZq(q)]);
-                f[q] = L->map[s] == ORC_WALL ? src[c * NQ + OPP(q)] : src[s * NQ + q];
-            }
-        } else {
-            pull(L, src, xs, ys, zs, f);
-        }
+        pull(L, src, xs, ys, zs, f);
         double r[4];
         orc_density_velocity(f, fx, fy, fz, r);
         rho = r[0]; vx = r[1]; vy = r[2]; vz = r[3];

@@ -67,7 +67,9 @@ typedef struct {
     int collision;
     int equilibrium;
     int cy_mode;
-    int halfway_bounce_back; /* 0: wall nodes with full-way bounce-back (reference) */
+    int halfway_bounce_back; /* 0: wall nodes with full-way bounce-back (reference); 1: halfway:
+                                every pull from a WALL cell takes the pulling centre's own
+                                post-collision population of the opposite direction */
     double nu;               /* lattice viscosity (nu_inf when Carreau-Yasuda is on) */
     double cy_nu0, cy_lambda, cy_a, cy_n;
     double fx, fy, fz;       /* homogeneous body force */

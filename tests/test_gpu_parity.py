@@ -386,8 +386,16 @@ def test_watchdog_reports_density_out_of_range_and_recovers(dtype):
     good = orc.get_df()
     labels = orc.get_map()
     bad = good.copy()
-    z, y, x = [int(v[len(v) // 2]) for v in np.nonzero(labels == G.MAP_FLUID)]
-    bad[:, z, y, x] *= 5.0  # density 5 at one fluid cell
+    # a fluid cell whose 26 neighbours are fluid too: the next step pulls its populations from
+    # them, so all 27 cells are scaled to give it density 5
+    fl = labels == G.MAP_FLUID
+    inner = fl.copy()
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                inner &= np.roll(fl, (dz, dy, dx), axis=(0, 1, 2))
+    z, y, x = [int(v[len(v) // 2]) for v in np.nonzero(inner)]
+    bad[:, z - 1:z + 2, y - 1:y + 2, x - 1:x + 2] *= 5.0
     lat.import_df(bad)
     with pytest.raises(capi.NnlbmError) as e:
         lat.step(1)
@@ -406,3 +414,104 @@ def test_watchdog_reports_density_out_of_range_and_recovers(dtype):
     tol = FP64_TOL if dtype == "f64" else 1e-5
     fluid = labels == G.MAP_FLUID
     assert max_rel(lat.export_df()[:, fluid], orc.get_df()[:, fluid]) <= tol
+
+
+# -- halfway bounce-back (no reference counterpart; against the oracle's halfway mode) ----------
+def _halfway_pair(collision=0, dtype="f64", geometry="pipe", cy_mode=O.CY_NONE, cy=(0.0, 0.0, 2.0, 1.0), eq=O.EQ_INV_CUM_REF):
+    cyname = {0: "none", 1: "ref-fd", 2: "local-neq"}[cy_mode]
+    eqname = {v: k for k, v in capi.EQUILIBRIA.items()}[eq]
+    if geometry == "pipe":
+        m, prof = G.pipe_map(96, 32, 32, 12.0)
+        nz, ny, nx = m.shape
+        nu = 1.0 / 30.0
+        orc = O.Oracle(nx, ny, nz, collision=collision, equilibrium=eq, nu=nu, cy_mode=cy_mode, cy=cy, halfway=True)
+        orc.set_map(m)
+        orc.set_inflow_profile(G.expand_profile(m, prof) * 0.04)
+        lat = Lattice(CaseSpec((nx, ny, nz), collision=O.COLLISIONS[collision], dtype=dtype, equilibrium=eqname,
+                               cy_mode=cyname, nu=nu, cy=cy, bounce_back="halfway"))
+        lat.set_map(m)
+        lat.set_inflow_profile(prof * 0.04)
+    else:
+        wall = small_junction()
+        nz, ny, nx = wall.shape
+        orc = O.Oracle(nx, ny, nz, collision=collision, equilibrium=eq, nu=0.02, cy_mode=cy_mode, cy=cy, halfway=True)
+        rc, counts = orc.setup_tcpc(wall)
+        lat = Lattice(CaseSpec((nx, ny, nz), collision=O.COLLISIONS[collision], dtype=dtype, equilibrium=eqname,
+                               cy_mode=cyname, nu=0.02, cy=cy, bounce_back="halfway"))
+        lat.setup_tcpc(wall)
+        for L in (orc, lat):
+            L.set_inflow(ivc_flux=0.03 * counts[0], svc_flux=0.02 * counts[1])
+    return orc, lat
+
+
+def _live(labels):
+    """[27][z][y][x] True at the populations of every cell but the walls (with halfway
+    bounce-back nothing reads a wall cell's populations)."""
+    return np.broadcast_to(labels != G.MAP_WALL, (27,) + labels.shape)
+
+
+def test_fp64_halfway_pipe_configuration():
+    """The pipe configuration with the halfway bounce-back it names: both A-A layouts, then
+    100 steps."""
+    orc, lat = _halfway_pair()
+    for L in (orc, lat):
+        L.init_equilibrium()
+    live = _live(orc.get_map())
+    for n in (1, 2, 3, 94):
+        orc.step(n)
+        lat.step(n)
+        assert max_rel(lat.export_df()[live], orc.get_df()[live]) <= FP64_TOL, n
+
+
+@pytest.mark.parametrize("collision,eq", [(0, O.EQ_INV_CUM_REF), (10, O.EQ_DEFAULT), (4, O.EQ_INV_CUM_REF)],
+                         ids=["CUM", "BGK", "KBC_N4"])
+def test_fp64_halfway_junction(collision, eq):
+    """The TCPC junction: open-plane nodes finished by their inward neighbour and walls next to
+    the planes."""
+    orc, lat = _halfway_pair(collision, geometry="junction", eq=eq)
+    for L in (orc, lat):
+        L.init_equilibrium()
+    orc.step(100)
+    lat.step(100, macro=True)
+    live = _live(orc.get_map())
+    assert max_rel(lat.export_df()[live], orc.get_df()[live]) <= FP64_TOL
+
+
+def test_fp64_halfway_ref_fd_and_gathered_nodes():
+    """The finite-difference Carreau-Yasuda coupling: every open-plane node gathered by its own
+    kernel, and the velocity phase pulls next to walls."""
+    orc, lat = _halfway_pair(0, geometry="junction", cy_mode=O.CY_REF_FD, cy=CY)
+    for L in (orc, lat):
+        L.init_equilibrium()
+    orc.step(60)
+    lat.step(60, macro=True)
+    live = _live(orc.get_map())
+    assert max_rel(lat.export_df()[live], orc.get_df()[live]) <= FP64_TOL
+
+
+def test_fp64_halfway_moving_initial_state_and_import():
+    orc, lat = _halfway_pair()
+    for L in (orc, lat):
+        L.init_equilibrium(1.0, 0.01, 0.004, -0.003)
+    live = _live(orc.get_map())
+    orc.step(7)
+    lat.step(7)
+    assert max_rel(lat.export_df()[live], orc.get_df()[live]) <= FP64_TOL
+    lat.import_df(orc.get_df())
+    assert max_rel(lat.export_df()[live], orc.get_df()[live]) == 0.0
+    orc.step(9)
+    lat.step(9)
+    assert max_rel(lat.export_df()[live], orc.get_df()[live]) <= FP64_TOL
+
+
+def test_fp32_halfway_pipe_vs_fp64_oracle():
+    orc, lat = _halfway_pair(dtype="f32")
+    for L in (orc, lat):
+        L.init_equilibrium()
+    orc.step(200)
+    lat.step(200, macro=True)
+    fluid = orc.get_map() == G.MAP_FLUID
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
+    for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
+        assert err <= 2e-5, err
