@@ -575,19 +575,127 @@ template <> struct Cook<3> {
     __device__ static __forceinline__ float get(__nv_bfloat16 v) { return __bfloat162float(v); }
 };
 
+// ---------------------------------------------------------------------------------------
+// x-adjacent pairs: where a pair of chunks is one contiguous 64-cell row span whose cells
+// all collide, lane l takes cells 2l and 2l+1, so that one 4-byte (FP16, BF16) or 8-byte
+// (FP32) access moves a population of both and feeds the f2 pair with one conversion.  A pair
+// of elements that starts at an odd element (the odd step's +-1 shifts in x) is put together
+// from the aligned pairs around it with a shuffle: each lane reads (e+1, e+2) and takes e from
+// the lane before; stores write the aligned pairs between the lanes' values and the two
+// elements at the ends of the span alone (their neighbours belong to other spans).
+// ---------------------------------------------------------------------------------------
+template <int DT> struct Pair2;
+template <> struct Pair2<1> {
+    __device__ static __forceinline__ f2 load(const float* e) { return f2(*(const float2*)e); }
+    __device__ static __forceinline__ void store(float* e, f2 v) { *(float2*)e = v.v; }
+};
+template <> struct Pair2<2> {
+    __device__ static __forceinline__ f2 of(unsigned w)
+    {
+        const __half2 h = *reinterpret_cast<const __half2*>(&w);
+        return f2(__half22float2(h));
+    }
+    __device__ static __forceinline__ unsigned word(f2 v)
+    {
+        const __half2 h = __float22half2_rn(v.v);
+        return *reinterpret_cast<const unsigned*>(&h);
+    }
+};
+template <> struct Pair2<3> {
+    __device__ static __forceinline__ f2 of(unsigned w)
+    {
+        const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162*>(&w);
+        return f2(__bfloat1622float2(h));
+    }
+    __device__ static __forceinline__ unsigned word(f2 v)
+    {
+        const __nv_bfloat162 h = __float22bfloat162_rn(v.v);
+        return *reinterpret_cast<const unsigned*>(&h);
+    }
+};
+
+// elements (e, e+1) of every lane, e = base + 2 lane; `aligned`: e is an even element
+template <int DT>
+__device__ __forceinline__ f2 load_adjacent(const typename Storage<DT>::T* e, bool aligned, int lane)
+{
+    if constexpr (DT == 1) {
+        if (aligned) return Pair2<1>::load(e);
+        const float2 w = *(const float2*)(e + 1);
+        float lo = __shfl_up_sync(0xffffffffu, w.y, 1);
+        if (lane == 0) lo = e[0];
+        return f2(lo, w.x);
+    } else {
+        if (aligned) return Pair2<DT>::of(*(const unsigned*)e);
+        const unsigned w = *(const unsigned*)(e + 1);
+        unsigned prev = __shfl_up_sync(0xffffffffu, w, 1);
+        if (lane == 0) prev = *(const unsigned*)(e - 1);
+        return Pair2<DT>::of(__byte_perm(prev, w, 0x5432));
+    }
+}
+
+template <int DT>
+__device__ __forceinline__ void store_adjacent(typename Storage<DT>::T* e, f2 v, bool aligned, int lane)
+{
+    if constexpr (DT == 1) {
+        if (aligned) { Pair2<1>::store(e, v); return; }
+        const float nxt = __shfl_down_sync(0xffffffffu, v.v.x, 1);
+        if (lane < 31) *(float2*)(e + 1) = make_float2(v.v.y, nxt);
+        if (lane == 0) e[0] = v.v.x;
+        if (lane == 31) e[1] = v.v.y;
+    } else {
+        const unsigned mine = Pair2<DT>::word(v);
+        if (aligned) { *(unsigned*)e = mine; return; }
+        const unsigned nxt = __shfl_down_sync(0xffffffffu, mine, 1);
+        if (lane < 31) *(unsigned*)(e + 1) = __byte_perm(mine, nxt, 0x5432);
+        unsigned short* h = (unsigned short*)e;
+        if (lane == 0) h[0] = (unsigned short)(mine & 0xffffu);
+        if (lane == 31) h[1] = (unsigned short)(mine >> 16);
+    }
+}
+
+// whether the element at slot base p + c0 starts an aligned pair
+template <int DT>
+__device__ __forceinline__ bool pair_aligned(const void* p, int c0)
+{
+    return (((uintptr_t)((const typename Storage<DT>::T*)p + c0)) & (2 * sizeof(typename Storage<DT>::T) - 1)) == 0;
+}
+
+// two chunks that are one contiguous 64-cell span of colliding cells with no node to serve
+template <int DT>
+__device__ __forceinline__ bool adjacent_span(const Chunk& ca, const Chunk& cb)
+{
+    return DT != 0 && (ca.fluid & cb.fluid) == 0xffffffffu && cb.c0 == ca.c0 + 32 && !(ca.c0 & 1) &&
+           !((ca.cflags | cb.cflags) & CH_SRC);
+}
+
+template <int DT, bool ODD>
+__device__ __forceinline__ void pair_load_adjacent(const CaseArgs<float>& a, int c0, int lane, f2* f)
+{
+    using T = typename Storage<DT>::T;
+    const f2 isc(a.inv_scale);
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const void* p = ODD ? a.slot_odd_ld[q] : a.slot_even[q];
+        const f2 raw = load_adjacent<DT>((const T*)p + c0 + 2 * lane, !ODD || pair_aligned<DT>(p, c0), lane);
+        const f2 w(weight<float>(q));
+        f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
+    }
+}
+
 // the rest of a pair once its populations f (raw stored value + weight, or the rest state
-// where the cell does not collide) are in registers: collision, stores, per-cell outputs
+// where the cell does not collide) are in registers: collision, stores, per-cell outputs.
+// `adj`: an x-adjacent span (lane l holds cells c0 + 2l and c0 + 2l + 1)
 template <int DT, int COL, bool ODD>
 __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const CaseArgs<float>* ap, const Chunk& ca,
-                                            const Chunk& cb, const Chunk* cap, f2* f, int step, int flags, int lane)
+                                            const Chunk& cb, const Chunk* cap, f2* f, int step, int flags, int lane, bool adj)
 {
     using T = typename Storage<DT>::T;
     const unsigned bit = 1u << lane;
-    const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
+    const bool fa = adj || (ca.fluid & bit) != 0, fb = adj || (cb.fluid & bit) != 0;
     double mass = 0.0;
     float r[2] = {1.f, 1.f}, u0[2] = {0.f, 0.f}, u1[2] = {0.f, 0.f}, u2[2] = {0.f, 0.f};
     if (fa || fb) {
-        const int cA = ca.c0 + lane, cB = cb.c0 + lane;
+        const int cA = adj ? ca.c0 + 2 * lane : ca.c0 + lane, cB = adj ? ca.c0 + 2 * lane + 1 : cb.c0 + lane;
         const f2 fx(a.fx), fy(a.fy), fz(a.fz);
         f2 rho, ux, uy, uz;
         density_velocity<f2>(f, fx, fy, fz, rho, ux, uy, uz);
@@ -602,8 +710,12 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Case
             T* p = (T*)(ODD ? a.slot_odd_st[q] : a.slot_even[oppq(q)]);
             const f2 w(weight<float>(q));
             const f2 v = DT == 1 ? f[q] - w : mad(f[q], sc, -(w * sc));
-            if (fa) p[cA] = Cook<DT>::put(v.v.x);
-            if (fb) p[cB] = Cook<DT>::put(v.v.y);
+            if (adj) {
+                store_adjacent<DT>(p + cA, v, !ODD || pair_aligned<DT>(p, ca.c0), lane);
+            } else {
+                if (fa) p[cA] = Cook<DT>::put(v.v.x);
+                if (fb) p[cB] = Cook<DT>::put(v.v.y);
+            }
         }
         r[0] = rho.v.x; r[1] = rho.v.y; u0[0] = ux.v.x; u0[1] = ux.v.y;
         u1[0] = uy.v.x; u1[1] = uy.v.y; u2[0] = uz.v.x; u2[1] = uz.v.y;
@@ -721,8 +833,10 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
             const CaseArgs<CT>& a = case_args<ARGS>(g, ci);
             if (pairable<ARGS>(g, ca, cb)) {
                 f2 f[27];
-                pair_load<DT, ODD>(a, ca, cb, lane, f);
-                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, g.chunks + 2 * w, f, step, flags, lane);
+                const bool adj = adjacent_span<DT>(ca, cb);
+                if (adj) pair_load_adjacent<DT, ODD>(a, ca.c0, lane, f);
+                else pair_load<DT, ODD>(a, ca, cb, lane, f);
+                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, g.chunks + 2 * w, f, step, flags, lane, adj);
             } else {
                 fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, g.chunks + 2 * w, step, flags, lane);
                 if (cb.fluid) {

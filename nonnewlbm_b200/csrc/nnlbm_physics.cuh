@@ -167,15 +167,26 @@ __device__ __forceinline__ void fwd3(CT m, CT z, CT p, CT u, CT& k0, CT& k1, CT&
     k2 = mad(u * u, k0, mad(-(CT(2) * u), d, s));
 }
 
+// the coefficients of one axis of the backward transform:
+// z = k0 (1-u^2) - 2u k1 - k2, m = k0 (u^2-u)/2 + k1 (u - 1/2) + k2/2,
+// p = k0 (u^2+u)/2 + k1 (u + 1/2) + k2/2
 template <class CT>
-__device__ __forceinline__ void bwd3(CT k0, CT k1, CT k2, CT u, CT& m, CT& z, CT& p)
+struct Bwd {
+    CT a, b, c, d, e, ntu;
+    __device__ __forceinline__ explicit Bwd(CT u)
+    {
+        const CT uu = u * u;
+        a = CT(1) - uu; b = CT(0.5) * (uu - u); c = u - CT(0.5); d = CT(0.5) * (uu + u); e = u + CT(0.5); ntu = CT(-2) * u;
+    }
+};
+
+template <class CT>
+__device__ __forceinline__ void bwd3(CT k0, CT k1, CT k2, const Bwd<CT>& w, CT& m, CT& z, CT& p)
 {
-    // z = k0 (1-u^2) - 2u k1 - k2, m = (k0 (u^2-u) + k1 (2u-1) + k2)/2,
-    // p = (k0 (u^2+u) + k1 (2u+1) + k2)/2
-    const CT uu = u * u, tu = CT(2) * u;
-    z = mad(-tu, k1, k0 * (CT(1) - uu)) - k2;
-    m = (mad(k1, tu - CT(1), k0 * (uu - u)) + k2) * CT(0.5);
-    p = (mad(k1, tu + CT(1), k0 * (uu + u)) + k2) * CT(0.5);
+    const CT h = CT(0.5) * k2;
+    z = mad(k0, w.a, mad(w.ntu, k1, -k2));
+    m = mad(k0, w.b, mad(k1, w.c, h));
+    p = mad(k0, w.d, mad(k1, w.e, h));
 }
 
 template <class CT>
@@ -252,22 +263,32 @@ __device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, 
     s[2][1][1] = s211; s[1][2][1] = s121; s[1][1][2] = s112;
     s[2][2][0] = s220; s[0][2][2] = s022; s[2][0][2] = s202;
     s[2][2][2] = s222;
-    // backward: x, y, z (G2015 Eq 88-96)
+    // backward: x, y, z (G2015 Eq 88-96), each axis's coefficients made just before its pass
+    {
+        const Bwd<CT> wx(ux);
 #pragma unroll
-    for (int ky = 0; ky < 3; ++ky)
+        for (int ky = 0; ky < 3; ++ky)
 #pragma unroll
-        for (int kz = 0; kz < 3; ++kz)
-            bwd3<CT>(s[0][ky][kz], s[1][ky][kz], s[2][ky][kz], ux, b[0][ky][kz], b[1][ky][kz], b[2][ky][kz]);
+            for (int kz = 0; kz < 3; ++kz)
+                bwd3<CT>(s[0][ky][kz], s[1][ky][kz], s[2][ky][kz], wx, b[0][ky][kz], b[1][ky][kz], b[2][ky][kz]);
+    }
+    {
+        const Bwd<CT> wy(uy);
 #pragma unroll
-    for (int ix = 0; ix < 3; ++ix)
+        for (int ix = 0; ix < 3; ++ix)
 #pragma unroll
-        for (int kz = 0; kz < 3; ++kz)
-            bwd3<CT>(b[ix][0][kz], b[ix][1][kz], b[ix][2][kz], uy, a[ix][0][kz], a[ix][1][kz], a[ix][2][kz]);
+            for (int kz = 0; kz < 3; ++kz)
+                bwd3<CT>(b[ix][0][kz], b[ix][1][kz], b[ix][2][kz], wy, a[ix][0][kz], a[ix][1][kz], a[ix][2][kz]);
+    }
+    {
+        const Bwd<CT> wz(uz);
 #pragma unroll
-    for (int ix = 0; ix < 3; ++ix)
+        for (int ix = 0; ix < 3; ++ix)
 #pragma unroll
-        for (int iy = 0; iy < 3; ++iy)
-            bwd3<CT>(a[ix][iy][0], a[ix][iy][1], a[ix][iy][2], uz, f[9 * ix + 3 * iy], f[9 * ix + 3 * iy + 1], f[9 * ix + 3 * iy + 2]);
+            for (int iy = 0; iy < 3; ++iy)
+                bwd3<CT>(a[ix][iy][0], a[ix][iy][1], a[ix][iy][2], wz, f[9 * ix + 3 * iy], f[9 * ix + 3 * iy + 1],
+                         f[9 * ix + 3 * iy + 2]);
+    }
 }
 
 // ---------------------------------------------------------------------------------------

@@ -515,3 +515,32 @@ def test_fp32_halfway_pipe_vs_fp64_oracle():
     for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
         err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
         assert err <= 2e-5, err
+
+
+@pytest.mark.parametrize("nx", [130, 131])
+@pytest.mark.parametrize("dtype,tol_u", [("f32", 2e-5), ("f16", 2e-3), ("bf16", 2e-2)])
+def test_adjacent_spans_vs_fp64_oracle(nx, dtype, tol_u):
+    """Full 64-cell spans of a periodic box collide as x-adjacent pairs (one 4- or 8-byte access
+    moves a population of two cells).  With nx = 131 the rows start at alternating element
+    parity, so the odd step's shifted accesses of some directions begin at odd elements and
+    are put together across lanes.  Velocity against the FP64 oracle after 200 steps,
+    relative to the peak velocity."""
+    m, prof = G.dense_box_map(nx, 6, 5)
+    nz, ny, _ = m.shape
+    orc = O.Oracle(nx, ny, nz, collision=0, nu=0.05 / 3)
+    lat = Lattice(CaseSpec((nx, ny, nz), collision="CUM", dtype=dtype, nu=0.05 / 3))
+    lat.set_launch(128, 2)
+    orc.set_map(m)
+    orc.set_inflow_profile(G.expand_profile(m, prof) * 0.05)
+    lat.set_map(m)
+    lat.set_inflow_profile(prof * 0.05)
+    for L in (orc, lat):
+        L.init_equilibrium()
+    for n in (1, 199):
+        orc.step(n)
+        lat.step(n, macro=True)
+    inner = m != G.MAP_INFLOW_EQ
+    umax = np.max(np.abs(orc.get_macro(O.M_VX)[inner]))
+    for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
+        err = np.max(np.abs(lat.macro(fl)[inner] - orc.get_macro(fo)[inner])) / umax
+        assert err <= tol_u, (fo, err)
