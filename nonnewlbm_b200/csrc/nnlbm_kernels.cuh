@@ -271,10 +271,14 @@ __device__ __forceinline__ void store_node_eq(const CaseArgs<typename Storage<DT
 #pragma unroll
         for (int q = 0; q < 27; ++q) S::store(qptr<DT>(a, oppq(q)), c, q, f[q], a.scale);
     } else {
+        // with halfway bounce-back a population headed into a wall stays in the node's slot opp(q)
+        const uint32_t hwm = a.hw ? a.hw[c] : 0u;
 #pragma unroll
-        for (int q = 0; q < 27; ++q)
-            S::store(qptr<DT>(a, q), wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz), q, f[q],
-                     a.scale);
+        for (int q = 0; q < 27; ++q) {
+            if ((hwm >> q) & 1u) S::store(qptr<DT>(a, oppq(q)), c, q, f[q], a.scale);
+            else S::store(qptr<DT>(a, q), wrapc(x + cxq(q), a.nx) + sy * wrapc(y + cyq(q), a.ny) + sz * wrapc(z + czq(q), a.nz),
+                          q, f[q], a.scale);
+        }
     }
 }
 
@@ -372,9 +376,10 @@ __device__ __noinline__ void serve_nodes(const CaseArgs<typename Storage<DT>::CT
             served_state<CT>(lab, rho, ux, uy, uz, ctl, r, u, v, w);
             CT f[27];
             equilibrium<CT>(a.eq, r, u, v, w, f);
+            const uint32_t hwm = (ODD && a.hw) ? a.hw[n] : 0u; // halfway: populations headed into a wall stay
 #pragma unroll
             for (int q = 0; q < 27; ++q) {
-                if (!ODD) S::store((T*)a.slot_even[oppq(q)], n, q, f[q], a.scale);
+                if (!ODD || ((hwm >> q) & 1u)) S::store((T*)a.slot_even[oppq(q)], n, q, f[q], a.scale);
                 else S::store((T*)a.slot_odd_st[q], n + node_wrap(xn, yn, z, q, a.nx, a.ny, a.nz), q, f[q], a.scale);
             }
             served_outputs<CT>(a, flags, lab, n, r, u, v, w);
@@ -396,7 +401,8 @@ __device__ __noinline__ void serve_nodes(const CaseArgs<typename Storage<DT>::CT
             if (lane < 27) {
                 const int q = lane;
                 const CT fq = feq_one<CT>(a.eq, q, r, u, v, w);
-                if (!ODD) S::store((T*)a.slot_even[oppq(q)], n, q, fq, a.scale);
+                const bool stay = ODD && a.hw && ((a.hw[n] >> q) & 1u); // halfway: headed into a wall
+                if (!ODD || stay) S::store((T*)a.slot_even[oppq(q)], n, q, fq, a.scale);
                 else S::store((T*)a.slot_odd_st[q], n + node_wrap(xn, yn, z, q, a.nx, a.ny, a.nz), q, fq, a.scale);
             }
             if (lane == s) served_outputs<CT>(a, flags, lab, n, r, u, v, w);

@@ -505,6 +505,8 @@ def test_fp64_halfway_moving_initial_state_and_import():
 
 
 def test_fp32_halfway_pipe_vs_fp64_oracle():
+    """FP32 storage with halfway walls against the FP64 oracle after 200 steps: velocity within
+    5e-5 of the peak (the pipe's inlet peak is 0.04)."""
     orc, lat = _halfway_pair(dtype="f32")
     for L in (orc, lat):
         L.init_equilibrium()
@@ -514,17 +516,44 @@ def test_fp32_halfway_pipe_vs_fp64_oracle():
     umax = np.max(np.abs(orc.get_macro(O.M_VX)[fluid]))
     for fo, fl in ((O.M_VX, capi.M_VX), (O.M_VY, capi.M_VY), (O.M_VZ, capi.M_VZ)):
         err = np.max(np.abs(lat.macro(fl)[fluid] - orc.get_macro(fo)[fluid])) / umax
-        assert err <= 2e-5, err
+        assert err <= 5e-5, err
+
+
+def _adjacent_box(nx, dtype, cells_per_thread):
+    m, prof = G.dense_box_map(nx, 6, 5)
+    nz, ny, _ = m.shape
+    lat = Lattice(CaseSpec((nx, ny, nz), collision="CUM", dtype=dtype, nu=0.05 / 3))
+    lat.set_launch(128, cells_per_thread)
+    lat.set_map(m)
+    lat.set_inflow_profile(prof * 0.05)
+    lat.init_equilibrium()
+    return m, lat
 
 
 @pytest.mark.parametrize("nx", [130, 131])
-@pytest.mark.parametrize("dtype,tol_u", [("f32", 2e-5), ("f16", 2e-3), ("bf16", 2e-2)])
+def test_adjacent_spans_match_one_cell_form(nx):
+    """The paired form, whose full 64-cell spans collide as x-adjacent pairs (one 8-byte access
+    moves a population of two cells; with nx = 131 some odd-step accesses begin at odd elements
+    and are put together across lanes), against the one-cell form after 1, 2 and 5 FP32 steps:
+    the two differ only in rounding (packed against scalar arithmetic), 1e-5 relative per
+    population; a misplaced element would differ by the populations' spread."""
+    m, paired = _adjacent_box(nx, "f32", 2)
+    _, single = _adjacent_box(nx, "f32", 1)
+    live = np.broadcast_to(m != G.MAP_INFLOW_EQ, (27,) + m.shape)
+    for n in (1, 1, 3):
+        paired.step(n)
+        single.step(n)
+        assert max_rel(paired.export_df()[live], single.export_df()[live]) <= 1e-5, n
+
+
+@pytest.mark.parametrize("nx", [130, 131])
+@pytest.mark.parametrize("dtype,tol_u", [("f32", 5e-5), ("f16", 5e-3), ("bf16", 2e-2)])
 def test_adjacent_spans_vs_fp64_oracle(nx, dtype, tol_u):
     """Full 64-cell spans of a periodic box collide as x-adjacent pairs (one 4- or 8-byte access
     moves a population of two cells).  With nx = 131 the rows start at alternating element
     parity, so the odd step's shifted accesses of some directions begin at odd elements and
     are put together across lanes.  Velocity against the FP64 oracle after 200 steps,
-    relative to the peak velocity."""
+    relative to the peak velocity 0.05 (tau = 0.55, the least viscous flow of these tests)."""
     m, prof = G.dense_box_map(nx, 6, 5)
     nz, ny, _ = m.shape
     orc = O.Oracle(nx, ny, nz, collision=0, nu=0.05 / 3)
