@@ -123,6 +123,7 @@ struct Case {
     std::vector<uint8_t> label;      // plain solver labels
     std::vector<uint8_t> dlabel;     // labels with the work flags of the device copy
     std::vector<Chunk> chunks;       // work list (case index 0)
+    std::vector<ChunkNodes> chunk_nodes; // the open-plane nodes each chunk serves
     std::vector<int32_t> self_cell;  // cells handled by their own thread, in cell order
     std::vector<int32_t> gather_self;// self indices of the gathered nodes
     std::vector<double> self_prof;   // [n_self][3] prescribed velocity of INFLOW_EQ nodes
@@ -144,6 +145,7 @@ struct Group {
     bool dirty = true;
     void* d_cases = nullptr;         // CaseArgs<CT>[n]
     Chunk* d_chunks = nullptr;
+    ChunkNodes* d_chunk_nodes = nullptr;
     int n_chunks = 0;
     int4* d_gather = nullptr;
     int2* d_nodes = nullptr;
@@ -320,6 +322,7 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     // per-case argument array and the concatenated work lists of the group
     std::vector<CaseArgs<CT>> ca;
     std::vector<Chunk> chunks;
+    std::vector<ChunkNodes> chunk_nodes;
     std::vector<int4> gather;
     std::vector<int2> nodes;
     std::vector<CT> prof;
@@ -333,15 +336,16 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
             ch.cflags = (int)j | (ch.cflags & ~CH_CASE_MASK);
             chunks.push_back(ch);
         }
+        chunk_nodes.insert(chunk_nodes.end(), c.chunk_nodes.begin(), c.chunk_nodes.end());
         // a paired step kernel takes chunks two by two: an odd count gets an empty chunk
         // (no colliding lane), so that no pair mixes two cases and the list length is even
         if (pairs_chunks(g.dtype, g.collision) && (c.chunks.size() & 1)) {
             Chunk none = chunks.back();
             none.fluid = 0;
             none.periodic = 0;
-            none.xneg = none.xpos = none.xreq = none.yneg = none.ypos = 0;
             none.cflags &= ~CH_SRC;
             chunks.push_back(none);
+            chunk_nodes.push_back(ChunkNodes{});
         }
         for (int32_t k : c.gather_self)
             gather.push_back(make_int4(c.self_cell[k], (int)j, (int)(self_off + k), (int)c.label[c.self_cell[k]]));
@@ -351,16 +355,20 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     }
     if (g.d_cases) cudaFree(g.d_cases);
     if (g.d_chunks) cudaFree(g.d_chunks);
+    if (g.d_chunk_nodes) cudaFree(g.d_chunk_nodes);
     if (g.d_gather) cudaFree(g.d_gather);
     if (g.d_nodes) cudaFree(g.d_nodes);
     g.d_nodes = nullptr;
     if (g.d_bc_prof) cudaFree(g.d_bc_prof);
     if (g.d_bc_buf) cudaFree(g.d_bc_buf);
-    g.d_cases = nullptr; g.d_chunks = nullptr; g.d_gather = nullptr; g.d_bc_prof = nullptr; g.d_bc_buf = nullptr;
+    g.d_cases = nullptr; g.d_chunks = nullptr; g.d_chunk_nodes = nullptr; g.d_gather = nullptr; g.d_bc_prof = nullptr; g.d_bc_buf = nullptr;
     CK(cudaMalloc(&g.d_cases, std::max<size_t>(ca.size(), 1) * sizeof(CaseArgs<CT>)));
     CK(cudaMemcpy(g.d_cases, ca.data(), ca.size() * sizeof(CaseArgs<CT>), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void**)&g.d_chunks, std::max<size_t>(chunks.size(), 1) * sizeof(Chunk)));
     if (!chunks.empty()) CK(cudaMemcpy(g.d_chunks, chunks.data(), chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+    CK(cudaMalloc((void**)&g.d_chunk_nodes, std::max<size_t>(chunk_nodes.size(), 1) * sizeof(ChunkNodes)));
+    if (!chunk_nodes.empty())
+        CK(cudaMemcpy(g.d_chunk_nodes, chunk_nodes.data(), chunk_nodes.size() * sizeof(ChunkNodes), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void**)&g.d_nodes, std::max<size_t>(nodes.size(), 1) * sizeof(int2)));
     if (!nodes.empty()) CK(cudaMemcpy(g.d_nodes, nodes.data(), nodes.size() * sizeof(int2), cudaMemcpyHostToDevice));
     CK(cudaMalloc((void**)&g.d_gather, std::max<size_t>(gather.size(), 1) * sizeof(int4)));
@@ -378,6 +386,7 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     ga.n_cases = (int)ca.size();
     ga.cases = (const CaseArgs<CT>*)g.d_cases;
     ga.chunks = g.d_chunks;
+    ga.chunk_nodes = g.d_chunk_nodes;
     ga.n_chunks = g.n_chunks;
     ga.gather = g.d_gather;
     ga.n_gather = g.n_gather;
@@ -826,6 +835,7 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
     // population rows (but not into the previous chunk), so that a short row segment fills
     // one chunk instead of straddling two and each row load touches as few sectors as it can
     std::vector<Chunk> chunks;
+    std::vector<ChunkNodes> chunk_nodes;
     auto collides = [&](size_t i) { return map[i] == L_FLUID || map[i] == L_PERIODIC; };
     const int align = 32 / kStorageBytes[c.d.dtype];
     for (int z = 0; z < nz; ++z)
@@ -835,6 +845,7 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 if (x0 >= nx) break;
                 x0 = std::max(x0 / align * align, end);
                 Chunk ch{};
+                ChunkNodes cn{};
                 ch.c0 = (int)id(x0, y, z);
                 ch.yz = y | (z << 16);
                 for (int x = x0; x < std::min(nx, x0 + kChunk); ++x) {
@@ -843,11 +854,11 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                     if (collides(i)) {
                         ch.fluid |= bit;
                         if (map[i] == L_PERIODIC) ch.periodic |= bit;
-                        if (serves[i] & kServeXneg) ch.xneg |= bit;
-                        if (serves[i] & kServeXpos) ch.xpos |= bit;
-                        if (serves[i] & kServeXreq) ch.xreq |= bit;
-                        if (serves[i] & kServeYneg) ch.yneg |= bit;
-                        if (serves[i] & kServeYpos) ch.ypos |= bit;
+                        if (serves[i] & kServeXneg) cn.xneg |= bit;
+                        if (serves[i] & kServeXpos) cn.xpos |= bit;
+                        if (serves[i] & kServeXreq) cn.xreq |= bit;
+                        if (serves[i] & kServeYneg) cn.yneg |= bit;
+                        if (serves[i] & kServeYpos) cn.ypos |= bit;
                         if (!hw.empty() && hw[i]) ch.cflags |= CH_HW;
                     }
                 }
@@ -856,13 +867,15 @@ int nnlbm_set_map(nnlbm_ctx* ctx, int ic, const uint8_t* map)
                 const bool face = y == 0 || y == ny - 1 || z == 0 || z == nz - 1;
                 const unsigned xface = (x0 == 0 ? 1u : 0u) | (nx - 1 - x0 < kChunk ? 1u << (nx - 1 - x0) : 0u);
                 const bool plain = !face && !(ch.fluid & xface) && !(ch.cflags & CH_HW);
-                const bool serving = (ch.xneg | ch.xpos | ch.yneg | ch.ypos) != 0;
+                const bool serving = (cn.xneg | cn.xpos | cn.yneg | cn.ypos) != 0;
                 ch.cflags |= CH_FLUID | (face ? CH_FACE : 0) | (plain ? CH_PLAIN : 0) | (serving ? CH_SRC : 0);
                 chunks.push_back(ch);
+                chunk_nodes.push_back(cn);
             }
     c.label.assign(map, map + c.N);
     c.dlabel = dl;
     c.chunks = chunks;
+    c.chunk_nodes = chunk_nodes;
     c.self_cell = self_cell;
     c.gather_self = gather_self;
     c.self_prof.assign(self_cell.size() * 3, 0.0);
@@ -1547,7 +1560,7 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
     for (Group& g : ctx->groups) {
         for (int p = 0; p < 2; ++p)
             if (g.graph[p]) cudaGraphExecDestroy(g.graph[p]);
-        void* ptrs[] = {g.d_cases, g.d_chunks, g.d_gather, g.d_nodes, g.d_bc_prof, g.d_bc_buf};
+        void* ptrs[] = {g.d_cases, g.d_chunks, g.d_chunk_nodes, g.d_gather, g.d_nodes, g.d_bc_prof, g.d_bc_buf};
         for (void* p : ptrs)
             if (p) cudaFree(p);
     }

@@ -122,14 +122,16 @@ struct CaseArgs {
 };
 
 // one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
-// and per lane (bit = lane) which cells collide, which of those are PERIODIC, and which
-// finish an open-plane node next to them (serve_nodes): the node at x-1 (IN_L), at x+1
-// (IN_R, or OUT_REQ where the lane is in xreq too), at y-1 (OUT_F), at y+1 (OUT_B)
+// and per lane (bit = lane) which cells collide and which of those are PERIODIC
 struct alignas(16) Chunk {
-    int c0, yz, cflags;
-    unsigned fluid, periodic;
-    unsigned xneg, xpos, xreq, yneg, ypos;
-    unsigned pad0, pad1;
+    int c0, yz, cflags, pad0;
+    unsigned fluid, periodic, pad1, pad2;
+};
+// per chunk (in a parallel array read only by serve_nodes): which lanes finish an open-plane
+// node next to them, the node at x-1 (IN_L), at x+1 (IN_R, or OUT_REQ where the lane is in
+// xreq too), at y-1 (OUT_F), at y+1 (OUT_B)
+struct alignas(16) ChunkNodes {
+    unsigned xneg, xpos, xreq, yneg, ypos, pad0, pad1, pad2;
 };
 // chunk flags (bits 16.. of cflags, the case index below).  CH_PLAIN: no neighbour of any
 // colliding lane wraps around the box (the chunk is off the y/z faces and has no
@@ -152,6 +154,7 @@ struct GroupArgs {
     int n_cases, pad2;
     const CaseArgs<CT>* cases;
     const Chunk* chunks;
+    const ChunkNodes* chunk_nodes;  // [n_chunks]
     int n_chunks, pad0;
     const int4* gather;        // {cell, case, node index, label} of the open-plane nodes
     int n_gather, n_nodes;
@@ -305,6 +308,12 @@ __device__ __forceinline__ double node_outputs(const CaseArgs<CT>& a, int flags,
 // node, lane q storing population q; where many serve (an outlet row), each lane writes its
 // own.
 
+// the chunks that serve nodes are few; their node code stays out of line unless the build
+// asks otherwise
+#ifndef NNLBM_SERVE_INLINE
+#define NNLBM_SERVE_INLINE __noinline__
+#endif
+
 // the node of serving lane direction d (0: x-1, 1: x+1, 2: y-1, 3: y+1) and its label
 __device__ __forceinline__ int served_label(int d, bool req)
 {
@@ -348,17 +357,18 @@ __device__ __forceinline__ void served_outputs(const CaseArgs<CT>& a, int flags,
 // called by the whole warp of a chunk with serving lanes (CH_SRC), after its stores; rho and
 // u are each lane's pre-collision values
 template <int DT, bool ODD>
-__device__ __noinline__ void serve_nodes(const CaseArgs<typename Storage<DT>::CT>* ap, const Chunk* chp, int lane,
-                                         typename Storage<DT>::CT rho, typename Storage<DT>::CT ux,
-                                         typename Storage<DT>::CT uy, typename Storage<DT>::CT uz, int step, int flags)
+__device__ NNLBM_SERVE_INLINE void serve_nodes(const CaseArgs<typename Storage<DT>::CT>* ap, const Chunk* chp,
+                                               const ChunkNodes* cnp, int lane, typename Storage<DT>::CT rho,
+                                               typename Storage<DT>::CT ux, typename Storage<DT>::CT uy,
+                                               typename Storage<DT>::CT uz, int step, int flags)
 {
     using S = Storage<DT>;
     using T = typename S::T;
     using CT = typename S::CT;
     const CaseArgs<CT>& a = *ap;
-    // the record is read again here rather than kept in registers through the collision
+    // the records are read here rather than kept in registers through the collision
     const int c0 = chp->c0, yz = chp->yz;
-    const unsigned xneg = chp->xneg, xpos = chp->xpos, xreq = chp->xreq, yneg = chp->yneg, ypos = chp->ypos;
+    const unsigned xneg = cnp->xneg, xpos = cnp->xpos, xreq = cnp->xreq, yneg = cnp->yneg, ypos = cnp->ypos;
     const int y = yz & 0xffff, z = yz >> 16;
     const int sy = a.nx, x0 = c0 - y * sy - z * sy * a.ny;
     const StepCtl<CT>& ctl = a.ctl[step];
@@ -455,17 +465,27 @@ __host__ __device__ constexpr bool pairs_chunks(int dt, int col)
 
 // register budget per thread of each step-kernel variant: FP64 arithmetic may use all
 // 255; the paired form (two cells per thread) gets NNLBM_PAIR_REGS (two 256-thread blocks
-// per SM); the one-cell form of a collision that can pair gets NNLBM_CHUNK_REGS (four
-// blocks); KBC, which never pairs, 128
+// per SM); the one-cell form of a collision that can pair gets NNLBM_CHUNK_REGS_F32 with
+// FP32 storage (80, the most that keeps three blocks: the step then spills almost nothing,
+// which outweighs the lost warps) and
+// NNLBM_CHUNK_REGS with FP16/BF16 storage (four blocks: the packed loads need fewer
+// registers, and the extra warps hide the conversions); KBC, which never pairs, 128
 #ifndef NNLBM_PAIR_REGS
 #define NNLBM_PAIR_REGS 128
 #endif
 #ifndef NNLBM_CHUNK_REGS
 #define NNLBM_CHUNK_REGS 64
 #endif
+#ifndef NNLBM_CHUNK_REGS_F32
+#define NNLBM_CHUNK_REGS_F32 80
+#endif
 template <int DT, int COL, bool PAIR>
 struct StepRegs {
-    static constexpr int value = DT == 0 ? 255 : !pairs_chunks(DT, COL) ? 128 : PAIR ? NNLBM_PAIR_REGS : NNLBM_CHUNK_REGS;
+    static constexpr int value = DT == 0                ? 255
+                                 : !pairs_chunks(DT, COL) ? 128
+                                 : PAIR                   ? NNLBM_PAIR_REGS
+                                 : DT == 1                ? NNLBM_CHUNK_REGS_F32
+                                                          : NNLBM_CHUNK_REGS;
 };
 
 // ---------------------------------------------------------------------------------------
@@ -478,7 +498,8 @@ struct StepRegs {
 // ---------------------------------------------------------------------------------------
 template <int DT, int COL, bool ODD>
 __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>::CT>& a, const CaseArgs<typename Storage<DT>::CT>* ap,
-                                            const Chunk& ch, const Chunk* chp, int step, int flags, int lane)
+                                            const Chunk& ch, const Chunk* chp, const ChunkNodes* cnp, int step, int flags,
+                                            int lane)
 {
     using S = Storage<DT>;
     using T = typename S::T;
@@ -552,7 +573,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         if (!(rho > CT(0.25) && rho < CT(4))) atomicOr(a.err, 1);
         mass = (double)rho;
     }
-    if (ch.cflags & CH_SRC) serve_nodes<DT, ODD>(ap, chp, lane, rho, ux, uy, uz, step, flags);
+    if (ch.cflags & CH_SRC) serve_nodes<DT, ODD>(ap, chp, cnp, lane, rho, ux, uy, uz, step, flags);
     if (flags & F_REDUCE) {
         const double s0 = warp_sum(mass);
         if (lane == 0 && s0 != 0.0) atomicAdd(red_stripe(a.red, global_warp()), s0);
@@ -693,7 +714,8 @@ __device__ __forceinline__ void pair_load_adjacent(const CaseArgs<float>& a, int
 // `adj`: an x-adjacent span (lane l holds cells c0 + 2l and c0 + 2l + 1)
 template <int DT, int COL, bool ODD>
 __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const CaseArgs<float>* ap, const Chunk& ca,
-                                            const Chunk& cb, const Chunk* cap, f2* f, int step, int flags, int lane, bool adj)
+                                            const Chunk& cb, const Chunk* cap, const ChunkNodes* cnp, f2* f, int step, int flags,
+                                            int lane, bool adj)
 {
     using T = typename Storage<DT>::T;
     const unsigned bit = 1u << lane;
@@ -744,7 +766,7 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Case
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-        if ((h ? cb : ca).cflags & CH_SRC) serve_nodes<DT, ODD>(ap, cap + h, lane, r[h], u0[h], u1[h], u2[h], step, flags);
+        if ((h ? cb : ca).cflags & CH_SRC) serve_nodes<DT, ODD>(ap, cap + h, cnp + h, lane, r[h], u0[h], u1[h], u2[h], step, flags);
     }
     if (flags & F_REDUCE) {
         const double s0 = warp_sum(mass);
@@ -842,12 +864,14 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
                 const bool adj = adjacent_span<DT>(ca, cb);
                 if (adj) pair_load_adjacent<DT, ODD>(a, ca.c0, lane, f);
                 else pair_load<DT, ODD>(a, ca, cb, lane, f);
-                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, g.chunks + 2 * w, f, step, flags, lane, adj);
+                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, g.chunks + 2 * w, g.chunk_nodes + 2 * w, f, step, flags, lane,
+                                          adj);
             } else {
-                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, g.chunks + 2 * w, step, flags, lane);
+                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, g.chunks + 2 * w, g.chunk_nodes + 2 * w, step, flags, lane);
                 if (cb.fluid) {
                     const int cj = cb.cflags & CH_CASE_MASK;
-                    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, g.chunks + 2 * w + 1, step, flags, lane);
+                    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, g.chunks + 2 * w + 1,
+                                              g.chunk_nodes + 2 * w + 1, step, flags, lane);
                 }
             }
         } else {
@@ -857,7 +881,7 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
         if (w < g.n_chunks) {
             const Chunk ch = g.chunks[w];
             const int ci = ch.cflags & CH_CASE_MASK;
-            fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, ci), g.cases + ci, ch, g.chunks + w, step, flags, lane);
+            fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, ci), g.cases + ci, ch, g.chunks + w, g.chunk_nodes + w, step, flags, lane);
         } else {
             node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
         }
