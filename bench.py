@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP16-storage, dense-box and 15-case batch measurements")
     ap.add_argument("--dense-warmup", type=int, default=200)
     ap.add_argument("--dense-steps", type=int, default=100)
+    ap.add_argument("--launch", default=None,
+                    help="block,cells_per_thread (e.g. 128,2) instead of the autotuned launch shape")
     return ap.parse_args()
 
 
@@ -454,7 +456,11 @@ def run_ours(a, dist: Dist) -> int:
     w = workload(a)
     lat = W.build_lattice(w, device=dev)
     info = lat.step_info()
-    lat.autotune(stats=stats)
+    if a.launch:
+        block, cpt = (int(v) for v in a.launch.split(","))
+        lat.set_launch(block, cpt)
+    else:
+        lat.autotune(stats=stats)
     lat.step(max(3, a.warmup), stats=stats)
     # the populations touched per step can be smaller than the 126 MB L2 (a sparse
     # junction), so every timed step starts from a cold L2

@@ -596,20 +596,71 @@ template <> struct Cook<1> {
 template <> struct Cook<2> {
     __device__ static __forceinline__ __half put(float v) { return __float2half_rn(v); }
     __device__ static __forceinline__ float get(__half v) { return __half2float(v); }
+    __device__ static __forceinline__ unsigned short bits(__half v) { return __half_as_ushort(v); }
+    __device__ static __forceinline__ float of_bits(unsigned short b) { return __half2float(__ushort_as_half(b)); }
 };
 template <> struct Cook<3> {
     __device__ static __forceinline__ __nv_bfloat16 put(float v) { return __float2bfloat16_rn(v); }
     __device__ static __forceinline__ float get(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ static __forceinline__ unsigned short bits(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
+    __device__ static __forceinline__ float of_bits(unsigned short b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
 };
+
+// predicated global loads (0 where `on` is false) and stores that stay one predicated
+// instruction each: a branch around each would split the warp's batch of loads, and its
+// stream of stores, into one piece per population
+__device__ __forceinline__ float ld_if(const float* p, bool on)
+{
+    float v = 0.f;
+    asm("{ .reg .pred q; setp.ne.b32 q, %2, 0; @q ld.global.f32 %0, [%1]; }" : "+f"(v) : "l"(p), "r"((int)on));
+    return v;
+}
+__device__ __forceinline__ unsigned short ld_if(const unsigned short* p, bool on)
+{
+    unsigned short v = 0;
+    asm("{ .reg .pred q; setp.ne.b32 q, %2, 0; @q ld.global.b16 %0, [%1]; }" : "+h"(v) : "l"(p), "r"((int)on));
+    return v;
+}
+__device__ __forceinline__ void st_if(float* p, float v, bool on)
+{
+    asm volatile("{ .reg .pred q; setp.ne.b32 q, %2, 0; @q st.global.f32 [%0], %1; }" ::"l"(p), "f"(v), "r"((int)on)
+                 : "memory");
+}
+__device__ __forceinline__ void st_if(float2* p, float2 v, bool on)
+{
+    asm volatile("{ .reg .pred q; setp.ne.b32 q, %3, 0; @q st.global.v2.f32 [%0], {%1, %2}; }" ::"l"(p), "f"(v.x),
+                 "f"(v.y), "r"((int)on)
+                 : "memory");
+}
+__device__ __forceinline__ void st_if(unsigned* p, unsigned v, bool on)
+{
+    asm volatile("{ .reg .pred q; setp.ne.b32 q, %2, 0; @q st.global.b32 [%0], %1; }" ::"l"(p), "r"(v), "r"((int)on)
+                 : "memory");
+}
+__device__ __forceinline__ void st_if(unsigned short* p, unsigned short v, bool on)
+{
+    asm volatile("{ .reg .pred q; setp.ne.b32 q, %2, 0; @q st.global.b16 [%0], %1; }" ::"l"(p), "h"(v), "r"((int)on)
+                 : "memory");
+}
+
+// one population of a pair half: load (the raw stored value as float, 0 where off) and store
+template <int DT>
+__device__ __forceinline__ float pair_get(const typename Storage<DT>::T* p, bool on)
+{
+    if constexpr (DT == 1) return ld_if(p, on);
+    else return Cook<DT>::of_bits(ld_if((const unsigned short*)p, on));
+}
+template <int DT>
+__device__ __forceinline__ void pair_put(typename Storage<DT>::T* p, float v, bool on)
+{
+    if constexpr (DT == 1) st_if(p, v, on);
+    else st_if((unsigned short*)p, Cook<DT>::bits(Cook<DT>::put(v)), on);
+}
 
 // ---------------------------------------------------------------------------------------
 // x-adjacent pairs: where a pair of chunks is one contiguous 64-cell row span whose cells
 // all collide, lane l takes cells 2l and 2l+1, so that one 4-byte (FP16, BF16) or 8-byte
-// (FP32) access moves a population of both and feeds the f2 pair with one conversion.  A pair
-// of elements that starts at an odd element (the odd step's +-1 shifts in x) is put together
-// from the aligned pairs around it with a shuffle: each lane reads (e+1, e+2) and takes e from
-// the lane before; stores write the aligned pairs between the lanes' values and the two
-// elements at the ends of the span alone (their neighbours belong to other spans).
+// (FP32) access moves a population of both and feeds the f2 pair with one conversion.
 // ---------------------------------------------------------------------------------------
 template <int DT> struct Pair2;
 template <> struct Pair2<1> {
@@ -641,50 +692,48 @@ template <> struct Pair2<3> {
     }
 };
 
-// elements (e, e+1) of every lane, e = base + 2 lane; `aligned`: e is an even element
-template <int DT>
-__device__ __forceinline__ f2 load_adjacent(const typename Storage<DT>::T* e, bool aligned, int lane)
+// elements (e, e+1) of every lane, e = base + 2 lane.  The even step's pairs start at an even
+// element and move as one 8-byte (FP32) or 4-byte (FP16, BF16) access.  The odd step's pairs
+// are shifted by the neighbour offsets, whose parity depends on the box width, and move as
+// their two elements (the warp's two accesses touch the same sectors): the access form is
+// then fixed at compile time, no population waits behind a branch on its alignment, and the
+// 27 loads issue as one batch
+template <int DT, bool SPLIT>
+__device__ __forceinline__ f2 load_adjacent(const typename Storage<DT>::T* e)
 {
     if constexpr (DT == 1) {
-        if (aligned) return Pair2<1>::load(e);
-        const float2 w = *(const float2*)(e + 1);
-        float lo = __shfl_up_sync(0xffffffffu, w.y, 1);
-        if (lane == 0) lo = e[0];
-        return f2(lo, w.x);
+        if constexpr (SPLIT) return f2(e[0], e[1]);
+        else return Pair2<1>::load(e);
     } else {
-        if (aligned) return Pair2<DT>::of(*(const unsigned*)e);
-        const unsigned w = *(const unsigned*)(e + 1);
-        unsigned prev = __shfl_up_sync(0xffffffffu, w, 1);
-        if (lane == 0) prev = *(const unsigned*)(e - 1);
-        return Pair2<DT>::of(__byte_perm(prev, w, 0x5432));
+        if constexpr (SPLIT) {
+            const unsigned short* h = (const unsigned short*)e;
+            return Pair2<DT>::of((unsigned)h[0] | ((unsigned)h[1] << 16));
+        } else {
+            return Pair2<DT>::of(*(const unsigned*)e);
+        }
     }
 }
 
-template <int DT>
-__device__ __forceinline__ void store_adjacent(typename Storage<DT>::T* e, f2 v, bool aligned, int lane)
+template <int DT, bool SPLIT>
+__device__ __forceinline__ void store_adjacent(typename Storage<DT>::T* e, f2 v)
 {
     if constexpr (DT == 1) {
-        if (aligned) { Pair2<1>::store(e, v); return; }
-        const float nxt = __shfl_down_sync(0xffffffffu, v.v.x, 1);
-        if (lane < 31) *(float2*)(e + 1) = make_float2(v.v.y, nxt);
-        if (lane == 0) e[0] = v.v.x;
-        if (lane == 31) e[1] = v.v.y;
+        if constexpr (SPLIT) {
+            e[0] = v.v.x;
+            e[1] = v.v.y;
+        } else {
+            Pair2<1>::store(e, v);
+        }
     } else {
-        const unsigned mine = Pair2<DT>::word(v);
-        if (aligned) { *(unsigned*)e = mine; return; }
-        const unsigned nxt = __shfl_down_sync(0xffffffffu, mine, 1);
-        if (lane < 31) *(unsigned*)(e + 1) = __byte_perm(mine, nxt, 0x5432);
-        unsigned short* h = (unsigned short*)e;
-        if (lane == 0) h[0] = (unsigned short)(mine & 0xffffu);
-        if (lane == 31) h[1] = (unsigned short)(mine >> 16);
+        const unsigned w = Pair2<DT>::word(v);
+        if constexpr (SPLIT) {
+            unsigned short* h = (unsigned short*)e;
+            h[0] = (unsigned short)(w & 0xffffu);
+            h[1] = (unsigned short)(w >> 16);
+        } else {
+            *(unsigned*)e = w;
+        }
     }
-}
-
-// whether the element at slot base p + c0 starts an aligned pair
-template <int DT>
-__device__ __forceinline__ bool pair_aligned(const void* p, int c0)
-{
-    return (((uintptr_t)((const typename Storage<DT>::T*)p + c0)) & (2 * sizeof(typename Storage<DT>::T) - 1)) == 0;
 }
 
 // two chunks that are one contiguous 64-cell span of colliding cells with no node to serve
@@ -703,7 +752,7 @@ __device__ __forceinline__ void pair_load_adjacent(const CaseArgs<float>& a, int
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const void* p = ODD ? a.slot_odd_ld[q] : a.slot_even[q];
-        const f2 raw = load_adjacent<DT>((const T*)p + c0 + 2 * lane, !ODD || pair_aligned<DT>(p, c0), lane);
+        const f2 raw = load_adjacent<DT, ODD>((const T*)p + c0 + 2 * lane);
         const f2 w(weight<float>(q));
         f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
     }
@@ -739,10 +788,10 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Case
             const f2 w(weight<float>(q));
             const f2 v = DT == 1 ? f[q] - w : mad(f[q], sc, -(w * sc));
             if (adj) {
-                store_adjacent<DT>(p + cA, v, !ODD || pair_aligned<DT>(p, ca.c0), lane);
+                store_adjacent<DT, ODD>(p + cA, v);
             } else {
-                if (fa) p[cA] = Cook<DT>::put(v.v.x);
-                if (fb) p[cB] = Cook<DT>::put(v.v.y);
+                pair_put<DT>(p + cA, v.v.x, fa);
+                pair_put<DT>(p + cB, v.v.y, fb);
             }
         }
         r[0] = rho.v.x; r[1] = rho.v.y; u0[0] = ux.v.x; u0[1] = ux.v.y;
@@ -787,7 +836,7 @@ __device__ __forceinline__ void pair_load(const CaseArgs<float>& a, const Chunk&
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
-        const f2 raw(fa ? Cook<DT>::get(p[cA]) : 0.f, fb ? Cook<DT>::get(p[cB]) : 0.f);
+        const f2 raw(pair_get<DT>(p + cA, fa), pair_get<DT>(p + cB, fb));
         const f2 w(weight<float>(q));
         f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
     }
