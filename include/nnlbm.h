@@ -35,8 +35,9 @@ typedef enum {
     NNLBM_ERR_ARG = -1,     /* invalid argument, label, size or state */
     NNLBM_ERR_CUDA = -2,    /* a CUDA runtime call failed */
     NNLBM_ERR_NAN = -3,     /* the device watchdog saw a non-finite or out-of-range density */
-    NNLBM_ERR_TIMEOUT = -4, /* reserved for a bounded device wait that gives up; no kernel of
-                               this library waits on another, so no call returns it today */
+    NNLBM_ERR_TIMEOUT = -4, /* a bounded device wait gave up: the staged step form waited too
+                               long (2 s) for its own bulk copies into shared memory; the
+                               states of the context are then undefined */
     NNLBM_ERR_OOM = -5,     /* device allocation failed */
     NNLBM_ERR_AREA = -6     /* zero inlet or outlet area after the TCPC boundary setup */
 } nnlbm_status;
@@ -253,8 +254,9 @@ int nnlbm_reduce(nnlbm_ctx* ctx, int ic, double* out5);
 
 /* Time the launch shapes of the step kernel on copies of the current state and keep the
  * fastest: the block size, and for the single-precision cumulant, BGK and MRT whether a
- * thread steps two cells (packed FP32) or one.  The two forms round differently, so
- * contexts that must agree bitwise should share the form (the default is two cells).
+ * thread steps two cells (packed FP32; plain or staged) or one.  The one- and two-cell
+ * forms round differently, so contexts that must agree bitwise should share the form (the
+ * default is two cells).
  * No reference counterpart (the reference takes --block-size, sim_tcpc.cu:118-119). */
 int nnlbm_autotune(nnlbm_ctx* ctx);
 
@@ -265,8 +267,16 @@ int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags);
 
 /* Set the step kernel's launch shape by hand for every launch group: `block` threads (64,
  * 128 or 256) and 1 or 2 cells a thread (2 applies to the single-precision cumulant, BGK
- * and MRT; the others step one).  Replaces --block-size (sim_tcpc.cu:118-119). */
+ * and MRT; the others step one).  2 | NNLBM_LAUNCH_STAGED selects the staged form of the
+ * two-cell kernel: persistent warps that bring each pair of chunks into shared memory with
+ * bulk copies while they collide the pair before (its block size is fixed at 128; results
+ * are bitwise those of the two-cell form).  Replaces --block-size (sim_tcpc.cu:118-119). */
+#define NNLBM_LAUNCH_STAGED 16
 int nnlbm_set_launch(nnlbm_ctx* ctx, int block, int cells_per_thread);
+
+/* The launch shape case ic's launch group runs with now (after nnlbm_autotune or
+ * nnlbm_set_launch): block size and cells a thread, as nnlbm_set_launch takes them. */
+int nnlbm_get_launch(nnlbm_ctx* ctx, int ic, int* block, int* cells_per_thread);
 
 /* Number of populations-kernel launches and bytes moved per step for case ic
  * (roofline bookkeeping). */

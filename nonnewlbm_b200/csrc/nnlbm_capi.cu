@@ -19,8 +19,9 @@
 
 namespace nnlbm {
 #define NNLBM_DECL_STEP(DT, COL)                                                                  \
-    void launch_step_##DT##_##COL(bool, bool, bool, dim3, dim3, cudaStream_t, const void*); \
-    cudaError_t load_step_##DT##_##COL();
+    void launch_step_##DT##_##COL(bool, bool, int, dim3, dim3, cudaStream_t, const void*); \
+    cudaError_t load_step_##DT##_##COL();                                                  \
+    int staged_blocks_##DT##_##COL();
 #define NNLBM_DECL_STEP_DT(DT)                                                                                        \
     NNLBM_DECL_STEP(DT, 0) NNLBM_DECL_STEP(DT, 1) NNLBM_DECL_STEP(DT, 2) NNLBM_DECL_STEP(DT, 3) NNLBM_DECL_STEP(DT, 4) \
     NNLBM_DECL_STEP(DT, 5) NNLBM_DECL_STEP(DT, 6) NNLBM_DECL_STEP(DT, 7) NNLBM_DECL_STEP(DT, 8) NNLBM_DECL_STEP(DT, 9) \
@@ -56,6 +57,16 @@ StepLauncher step_launcher(int dt, int col)
      launch_step_##DT##_4, launch_step_##DT##_5, launch_step_##DT##_6, launch_step_##DT##_7,             \
      launch_step_##DT##_8, launch_step_##DT##_9, launch_step_##DT##_10}
     static const StepLauncher table[4][11] = {NNLBM_ROW(0), NNLBM_ROW(1), NNLBM_ROW(2), NNLBM_ROW(3)};
+    return table[dt][col];
+}
+
+StagedOccupancy staged_occupancy(int dt, int col)
+{
+#define NNLBM_OROW(DT)                                                                                    \
+    {staged_blocks_##DT##_0, staged_blocks_##DT##_1, staged_blocks_##DT##_2, staged_blocks_##DT##_3,     \
+     staged_blocks_##DT##_4, staged_blocks_##DT##_5, staged_blocks_##DT##_6, staged_blocks_##DT##_7,     \
+     staged_blocks_##DT##_8, staged_blocks_##DT##_9, staged_blocks_##DT##_10}
+    static const StagedOccupancy table[4][11] = {NNLBM_OROW(0), NNLBM_OROW(1), NNLBM_OROW(2), NNLBM_OROW(3)};
     return table[dt][col];
 }
 
@@ -123,6 +134,7 @@ struct Case {
     std::vector<uint8_t> label;      // plain solver labels
     std::vector<uint8_t> dlabel;     // labels with the work flags of the device copy
     std::vector<Chunk> chunks;       // work list (case index 0)
+    bool stage_maps = false;         // the staged form's tensor maps are in args
     std::vector<ChunkNodes> chunk_nodes; // the open-plane nodes each chunk serves
     std::vector<int32_t> self_cell;  // cells handled by their own thread, in cell order
     std::vector<int32_t> gather_self;// self indices of the gathered nodes
@@ -157,6 +169,8 @@ struct Group {
     bool any_refd = false;
     int block = 256;
     bool paired = false;             // two cells a thread (set where the collision can pair)
+    bool staged = false;             // the paired form with staged loads (k_step_staged)
+    int staged_max_blocks = 0;       // resident blocks of k_step_staged on the device (0: no staged form)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint64_t graph_gen = ~0ull, gen = 0;
     ArgBytes<kGroupArgsBytes> args{}; // GroupArgs<CT>
@@ -185,6 +199,10 @@ struct nnlbm_ctx {
     char* d_status = nullptr;        // StatusLayout(cases.size()) on the device
     char* h_status = nullptr;        // its pinned host mirror
     bool status_fresh = false;       // the mirror holds the block as the last step left it
+    int sm_count = 0;
+    // the staged step's bounded waits (GroupArgs::stage_wait_ns, stage_pad)
+    long long stage_wait_ns = 2000000000LL;
+    int stage_pad = 0;
 };
 
 namespace {
@@ -208,8 +226,46 @@ int set_err(nnlbm_ctx* ctx, int code, const char* fmt, ...)
                            "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
     } while (0)
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library links only
+// the CUDA runtime); null where the driver does not offer it
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                 const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled()
+{
+    static EncodeTiled fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiled) nullptr;
+        }
+        return (EncodeTiled)p;
+    }();
+    return fn;
+}
+
+// the staged form's two tensor maps of a single-precision-arithmetic case (CaseArgs::tm_even,
+// tm_odd); false if they cannot be made (the case then never steps staged)
+template <int DT>
+bool encode_stage_maps(const Case& c, CUtensorMap* even, CUtensorMap* odd)
+{
+    using G = StageGeom<DT>;
+    const EncodeTiled enc = encode_tiled();
+    if (!enc) return false;
+    const CUtensorMapDataType type = DT == 1 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16;
+    const cuuint64_t dims[3] = {(cuuint64_t)c.q_stride, 9, 3};
+    const cuuint64_t strides[2] = {(cuuint64_t)c.q_stride * G::sz, (cuuint64_t)9 * c.q_stride * G::sz};
+    const cuuint32_t box_even[3] = {(cuuint32_t)G::win, 9, 3}, box_odd[3] = {(cuuint32_t)G::win, 1, 3}, one[3] = {1, 1, 1};
+    return enc(even, type, 3, c.df, dims, strides, box_even, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+           enc(odd, type, 3, c.df, dims, strides, box_odd, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class CT>
-void fill_case_args(const Case& c, CaseArgs<CT>& a)
+void fill_case_args(Case& c, CaseArgs<CT>& a)
 {
     memset(&a, 0, sizeof a);
     a.df = c.df;
@@ -237,6 +293,10 @@ void fill_case_args(const Case& c, CaseArgs<CT>& a)
         a.slot_odd_ld[q] = (const void*)(base + (uintptr_t)((oppq(q) * qs - sh) * S));
         a.slot_odd_st[q] = (const void*)(base + (uintptr_t)((q * qs + sh) * S));
     }
+    c.stage_maps = false;
+    if (c.df && c.d.dtype == NNLBM_F32) c.stage_maps = encode_stage_maps<1>(c, &a.tm_even, &a.tm_odd);
+    if (c.df && c.d.dtype == NNLBM_F16) c.stage_maps = encode_stage_maps<2>(c, &a.tm_even, &a.tm_odd);
+    if (c.df && c.d.dtype == NNLBM_BF16) c.stage_maps = encode_stage_maps<3>(c, &a.tm_even, &a.tm_odd);
 }
 
 void rebuild_case_args(nnlbm_ctx* ctx, Case& c)
@@ -395,6 +455,8 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     ga.bc_prof = (const CT*)g.d_bc_prof;
     ga.bc_buf = (CT*)g.d_bc_buf;
     ga.cursor = g.d_ints;
+    ga.stage_wait_ns = ctx->stage_wait_ns;
+    ga.stage_pad = ctx->stage_pad;
     g.dirty = false;
     g.gen++;
     return NNLBM_OK;
@@ -414,19 +476,47 @@ int step_warps(const Group& g)
     return std::max(cw + (int)((g.n_self + 31) / 32), 1);
 }
 
+// whether a group can step in the staged form: its collision pairs, the kernel fits on the
+// device, and every case has its tensor maps
+bool can_stage(const nnlbm_ctx* ctx, const Group& g)
+{
+    if (!pairs_chunks(g.dtype, g.collision) || g.staged_max_blocks <= 0) return false;
+    for (int ic : g.cases)
+        if (!ctx->cases[ic].stage_maps) return false;
+    return true;
+}
+
+// the step kernel's launch: the staged form runs persistent warps, as many blocks as stay
+// resident (or fewer, one warp per unit of work at most); the others one warp per unit
+struct StepShape {
+    dim3 grid, block;
+    int form;
+};
+StepShape step_shape(const Group& g)
+{
+    if (g.staged) {
+        const int per_block = kStagedThreads / kChunk;
+        const int blocks = std::max(1, std::min((step_warps(g) + per_block - 1) / per_block, g.staged_max_blocks));
+        return {dim3(blocks), dim3(kStagedThreads), FORM_STAGED};
+    }
+    const int per_block = g.block / kChunk;
+    return {dim3((step_warps(g) + per_block - 1) / per_block), dim3(g.block), g.paired ? FORM_PAIRED : FORM_ONE};
+}
+
 // enqueue one step of a group (no host synchronisation); `odd` is the A-A parity
 int enqueue_step(nnlbm_ctx* ctx, Group& g, bool odd)
 {
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
-    const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
+    const dim3 cblk(g.block);
+    const StepShape sh = step_shape(g);
     const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
     if (g.any_refd) {
         A.refd_velocity(odd, rgrid, cblk, ctx->stream, g.args.data());
         A.refd_stress(odd, rgrid, cblk, ctx->stream, g.args.data());
     }
     if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
-    step_launcher(g.dtype, g.collision)(odd, g.n_gather > 0, g.paired, cgrid, cblk, ctx->stream, g.args.data());
+    step_launcher(g.dtype, g.collision)(odd, g.n_gather > 0, sh.form, sh.grid, sh.block, ctx->stream, g.args.data());
     CK(cudaGetLastError());
     return NNLBM_OK;
 }
@@ -524,6 +614,10 @@ int check_watchdog(nnlbm_ctx* ctx)
 {
     const StatusLayout sl(ctx->cases.size());
     const int* err = (const int*)(ctx->h_status + sl.err);
+    for (size_t i = 0; i < ctx->cases.size(); ++i)
+        if (err[2 * i] & ERR_STALL)
+            return set_err(ctx, NNLBM_ERR_TIMEOUT, "case %zu: a staged step waited %.3f s for its bulk copies and gave up", i,
+                           ctx->stage_wait_ns * 1e-9);
     for (size_t i = 0; i < ctx->cases.size(); ++i)
         if (err[2 * i]) return set_err(ctx, NNLBM_ERR_NAN, "case %zu: density left (0.25, 4) or became non-finite", i);
     return NNLBM_OK;
@@ -743,11 +837,19 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
     }
     // load the kernels of every launch group and the module of nnlbm_step_noalloc's scratch
     // now, so that no later call loads code (and allocates) on first use
-    for (const Group& g : ctx->groups) {
+    CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+    for (Group& g : ctx->groups) {
         const cudaError_t e = load_group_kernels(g.dtype, g.collision);
         if (e != cudaSuccess)
             return set_err(ctx, NNLBM_ERR_CUDA, "loading the kernels of storage %d, collision %d failed: %s", g.dtype,
                            g.collision, cudaGetErrorString(e));
+        g.staged_max_blocks = staged_occupancy(g.dtype, g.collision)() * ctx->sm_count;
+    }
+    // a test's stall of the staged step: every wait expects 16 bytes that never arrive and
+    // gives up after a millisecond (NNLBM_ERR_TIMEOUT); all its copies still complete
+    if (const char* t = getenv("NNLBM_TEST_STAGE_STALL"); t && atoi(t) == 1) {
+        ctx->stage_wait_ns = 1000000LL;
+        ctx->stage_pad = 16;
     }
     char* scratch = nullptr;
     return noalloc_scratch(ctx, &scratch);
@@ -1321,15 +1423,20 @@ int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags)
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
-        // every launch shape: block size x (where the collision pairs) one or two cells a thread
+        // every launch shape: the staged form (fixed block), and block size x one or two cells
+        // a thread; the forms other than one cell a thread only where the collision pairs
         float best = 1e30f;
         int bb = g.block;
-        bool bp = g.paired;
-        const int n_forms = pairs_chunks(g.dtype, g.collision) ? 2 : 1;
-        for (int form = 0; form < n_forms; ++form) {
+        bool bp = g.paired, bs = g.staged;
+        const bool pairs = pairs_chunks(g.dtype, g.collision), stages = can_stage(ctx, g);
+        for (int form = FORM_STAGED; form >= FORM_ONE; --form) {
+            if ((form == FORM_PAIRED && !pairs) || (form == FORM_STAGED && !stages)) continue;
             for (int b : blocks) {
+                if (form == FORM_STAGED && b != blocks[0]) continue; // its block is fixed
                 g.block = b;
-                g.paired = n_forms == 2 && form == 0;
+                g.paired = form != FORM_ONE;
+                g.staged = form == FORM_STAGED;
+                g.gen++;
                 if ((rc = run_group_steps(ctx, g, 3, tf, false)) != NNLBM_OK) return rc;
                 CK(cudaEventRecord(e0, ctx->stream));
                 if ((rc = run_group_steps(ctx, g, 10, tf, false)) != NNLBM_OK) return rc;
@@ -1337,11 +1444,12 @@ int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags)
                 CK(cudaEventSynchronize(e1));
                 float ms = 0;
                 CK(cudaEventElapsedTime(&ms, e0, e1));
-                if (ms < best) { best = ms; bb = b; bp = g.paired; }
+                if (ms < best) { best = ms; bb = b; bp = g.paired; bs = g.staged; }
             }
         }
         g.block = bb;
         g.paired = bp;
+        g.staged = bs;
         g.gen++; // the graphs captured another launch shape
         for (size_t j = 0; j < g.cases.size(); ++j) {
             Case& c = ctx->cases[g.cases[j]];
@@ -1371,13 +1479,24 @@ int nnlbm_set_launch(nnlbm_ctx* ctx, int block, int cells_per_thread)
     if (!ctx) return NNLBM_ERR_ARG;
     if (block != 64 && block != 128 && block != 256)
         return set_err(ctx, NNLBM_ERR_ARG, "block size %d: use 64, 128 or 256", block);
-    if (cells_per_thread != 1 && cells_per_thread != 2)
-        return set_err(ctx, NNLBM_ERR_ARG, "cells per thread %d: use 1 or 2", cells_per_thread);
+    if (cells_per_thread != 1 && cells_per_thread != 2 && cells_per_thread != (2 | NNLBM_LAUNCH_STAGED))
+        return set_err(ctx, NNLBM_ERR_ARG, "cells per thread %d: use 1, 2 or 2 | NNLBM_LAUNCH_STAGED", cells_per_thread);
     for (Group& g : ctx->groups) {
         g.block = block;
-        g.paired = cells_per_thread == 2 && pairs_chunks(g.dtype, g.collision);
+        g.paired = (cells_per_thread & 2) && pairs_chunks(g.dtype, g.collision);
+        g.staged = (cells_per_thread & NNLBM_LAUNCH_STAGED) && can_stage(ctx, g);
         g.gen++; // the graphs captured another launch shape
     }
+    return NNLBM_OK;
+}
+
+int nnlbm_get_launch(nnlbm_ctx* ctx, int ic, int* block, int* cells_per_thread)
+{
+    int rc = check_case(ctx, ic);
+    if (rc) return rc;
+    const Group& g = ctx->groups[ctx->cases[ic].group];
+    if (block) *block = g.staged ? kStagedThreads : g.block;
+    if (cells_per_thread) *cells_per_thread = g.staged ? (2 | NNLBM_LAUNCH_STAGED) : g.paired ? 2 : 1;
     return NNLBM_OK;
 }
 
@@ -1407,7 +1526,7 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
     if ((rc = prepare_steps(ctx, g, n_steps, flags)) != NNLBM_OK) return rc;
     const AuxLaunchers& A = aux_launchers(g.dtype);
     const int per_block = g.block / kChunk;
-    const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
+    const dim3 cblk(g.block);
     const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
     for (int i = 0; i < 5; ++i) { ms[i] = 0; launches[i] = 0; }
     const int64_t parity = ctx->cases[g.cases[0]].parity;
@@ -1434,7 +1553,8 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
             A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, g.args.data());
             mark(0);
         }
-        step_launcher(g.dtype, g.collision)(odd, false, g.paired, cgrid, cblk, ctx->stream, g.args.data());
+        const StepShape sh = step_shape(g);
+        step_launcher(g.dtype, g.collision)(odd, false, sh.form, sh.grid, sh.block, ctx->stream, g.args.data());
         mark(1);
         CK(cudaGetLastError());
     }
@@ -1511,7 +1631,8 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         else noalloc_args<float>(g, gi, scratch, args);
         const AuxLaunchers& A = aux_launchers(g.dtype);
         const int per_block = g.block / kChunk;
-        const dim3 cgrid((step_warps(g) + per_block - 1) / per_block), cblk(g.block);
+        const dim3 cblk(g.block);
+        const StepShape sh = step_shape(g);
         const dim3 rgrid((std::max(g.n_chunks, 1) + per_block - 1) / per_block); // one warp per chunk
         const int64_t parity = ctx->cases[g.cases[0]].parity;
         for (int64_t k = 0; k < n_steps; ++k) {
@@ -1521,7 +1642,7 @@ int nnlbm_step_noalloc(nnlbm_ctx* ctx, int64_t n_steps, int flags)
                 A.refd_stress(odd, rgrid, cblk, ctx->stream, args);
             }
             if (g.n_gather > 0) A.gather(odd, dim3((g.n_gather + 63) / 64), dim3(64), ctx->stream, args);
-            step_launcher(g.dtype, g.collision)(odd, false, g.paired, cgrid, cblk, ctx->stream, args);
+            step_launcher(g.dtype, g.collision)(odd, false, sh.form, sh.grid, sh.block, ctx->stream, args);
         }
         CK(cudaGetLastError());
         finish_steps(ctx, g, n_steps, flags);

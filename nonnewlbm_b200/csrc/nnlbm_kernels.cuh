@@ -28,6 +28,7 @@
 // prescribed velocity and need no gather.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -119,6 +120,11 @@ struct CaseArgs {
     const void* slot_even[27];
     const void* slot_odd_ld[27];
     const void* slot_odd_st[27];
+    // the staged form's tensor maps of the population arrays (single-precision arithmetic
+    // only): dims {qstride cells, 9, 3} over slot s = 9 * hi + lo, boxes of StageGeom::win
+    // cells by {all 9 x all 3} (the even step's 27 slots of a chunk) and by {1 x all 3} (the
+    // three slots of one (cy, cz) group in the odd step)
+    CUtensorMap tm_even, tm_odd;
 };
 
 // one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
@@ -138,6 +144,9 @@ struct alignas(16) ChunkNodes {
 // colliding cell at x = 0 or nx-1); CH_SRC: some lane finishes an open-plane node
 enum : int { CH_CASE_MASK = 0xffff, CH_FLUID = 1 << 16, CH_FACE = 1 << 17, CH_PLAIN = 1 << 18, CH_SRC = 1 << 19,
              CH_HW = 1 << 20 };
+// bits of a case's watchdog word: a density out of range (or not finite), a bounded wait of
+// the staged step that gave up
+enum : int { ERR_DENSITY = 1, ERR_STALL = 2 };
 // CH_HW (halfway bounce-back): some colliding lane has a WALL neighbour; such chunks take the
 // general path, whose odd step reads a population arriving from a wall from the cell's own
 // slot q (where the previous, even, step left its f*_opp(q)) and stores a population leaving
@@ -165,6 +174,11 @@ struct GroupArgs {
     // cursor[p] and stores cursor[p] + 1 into cursor[1 - p], which no kernel of the step
     // reads, so no launch needs a grid-wide count
     int* cursor;
+    // the staged form's wait on its bulk copies gives up after stage_wait_ns and reports
+    // ERR_STALL; stage_pad (0 in a run) is added to the bytes each wait expects, so that a
+    // test can make every wait run out with all copies complete
+    long long stage_wait_ns;
+    int stage_pad, pad3;
 };
 
 // where a kernel finds the arguments of case ci: the device array, the parameters indexed
@@ -570,7 +584,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
             }
         }
         if (flags & F_STATS) accumulate_stats<CT>(a, c, rho, ux, uy, uz);
-        if (!(rho > CT(0.25) && rho < CT(4))) atomicOr(a.err, 1);
+        if (!(rho > CT(0.25) && rho < CT(4))) atomicOr(a.err, ERR_DENSITY);
         mass = (double)rho;
     }
     if (ch.cflags & CH_SRC) serve_nodes<DT, ODD>(ap, chp, cnp, lane, rho, ux, uy, uz, step, flags);
@@ -809,7 +823,7 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Case
                 }
             }
             if (flags & F_STATS) accumulate_stats<float>(a, cc[h], r[h], u0[h], u1[h], u2[h]);
-            if (!(r[h] > 0.25f && r[h] < 4.f)) atomicOr(a.err, 1);
+            if (!(r[h] > 0.25f && r[h] < 4.f)) atomicOr(a.err, ERR_DENSITY);
             mass += (double)r[h];
         }
     }
@@ -849,6 +863,22 @@ __device__ __forceinline__ bool pairable(const GroupArgs<float>& g, const Chunk&
     const int ci = ca.cflags & CH_CASE_MASK;
     return ((ca.cflags & cb.cflags) & CH_PLAIN) && ci == (cb.cflags & CH_CASE_MASK) &&
            case_args<ARGS>(g, ci).cy_mode != CY_REF_FD;
+}
+
+// a pair of chunks that does not collide as a pair, chunk by chunk.  Out of line, so that the
+// staged kernel's loop (the pair path) keeps a small instruction footprint and its
+// registers are allocated for the pair path alone
+template <int DT, int COL, bool ODD, int ARGS>
+__device__ __noinline__ void unpaired_chunks(const GroupArgs<float>& g, int u, int step, int flags, int lane)
+{
+    const Chunk ca = g.chunks[2 * u], cb = g.chunks[2 * u + 1];
+    const int ci = ca.cflags & CH_CASE_MASK;
+    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, ci), g.cases + ci, ca, g.chunks + 2 * u, g.chunk_nodes + 2 * u, step, flags, lane);
+    if (cb.fluid) {
+        const int cj = cb.cflags & CH_CASE_MASK;
+        fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, g.chunks + 2 * u + 1, g.chunk_nodes + 2 * u + 1, step,
+                                  flags, lane);
+    }
 }
 
 // 32 boundary nodes (open-plane nodes and GEO_INFLOW nodes, one per lane): each writes
@@ -934,6 +964,270 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
         } else {
             node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// the staged paired form: persistent warps, each stepping pairs of chunks in turn, whose
+// populations it has brought into shared memory with tensor copies (cp.async.bulk.tensor,
+// completion counted in bytes on an mbarrier) while it collided the pair before.  Each
+// warp owns two buffers and their barriers, so that no warp waits on another.  The loads
+// leave the warp's critical path (the copy of pair k + 1 is in flight while pair k
+// collides), and a population costs one or two shared-memory reads instead of a global load
+// and its address arithmetic.  One lane issues the copies: per chunk, the even step's 27
+// slots at the chunk's cells are one box; the odd step reads slot opp(q) at x - c_q, and the
+// three directions of one (cy, cz) share a row and differ by one cell in x, so each of the
+// nine (cy, cz) groups is one box a few cells wider than the chunk.  A box starts at the
+// 16-byte boundary at or below its first cell; the reads index it from that offset.  A pair
+// that is not pairable, and the boundary-node batches, take the unstaged paths.
+// ---------------------------------------------------------------------------------------
+template <int DT>
+struct StageGeom {
+    static constexpr int sz = (int)sizeof(typename Storage<DT>::T);
+    static constexpr int align = 16 / sz;                        // cells per 16 bytes
+    static constexpr int win = (32 + 2 + align - 1 + align - 1) / align * align; // box width: 40 (FP32), 48
+    static constexpr int row = win * sz;                          // one slot's window: 160 or 96 bytes
+    static constexpr int group = (3 * row + 127) / 128 * 128;     // an odd-step box, 128-byte aligned
+    static constexpr int chunk = 9 * group;                       // a chunk's 27 windows (>= 27 rows)
+    static constexpr int unit = 2 * chunk;                        // a pair
+    static constexpr unsigned tx = 54u * row;                     // bytes the boxes of a pair bring
+    static constexpr int warps = 4;                               // warps per block
+    static constexpr int smem = warps * 2 * unit + 128;           // two buffers per warp, alignment slack
+};
+constexpr int kStagedThreads = 128;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// the initialised barriers visible to the tensor-copy (async) proxy
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// one box of a 3-d tensor map into shared memory (x: the cell coordinate, a multiple of
+// 16 bytes; it may lie below zero or past the array, where the box reads zeros)
+__device__ __forceinline__ void tensor_to_smem(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    uint32_t ok;
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(ok)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// wait for the phase of `parity` to complete, for at most limit_ns (and at most 2^24 polls)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (int i = 0; i < (1 << 24); ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((long long)(global_ns() - t0) > limit_ns) break;
+    }
+    return false;
+}
+
+// the (cy, cz) of odd-step group lo (slot s = 9 hi + lo holds direction opp(s), whose
+// c = (hi - 1, lo / 3 - 1, lo % 3 - 1) negated)
+__device__ __forceinline__ int group_cy(int lo) { return 1 - lo / 3; }
+__device__ __forceinline__ int group_cz(int lo) { return 1 - lo % 3; }
+// the first cell of a chunk's window for odd-step group lo, before alignment: the source of
+// its first cell for cx = +1
+__device__ __forceinline__ int group_x0(const CaseArgs<float>& a, int c0, int lo)
+{
+    return c0 - group_cy(lo) * a.nx - group_cz(lo) * a.nx * a.ny - 1;
+}
+
+// one lane arms the barrier with the bytes of the pair and issues its boxes: one per chunk
+// (even step) or nine per chunk (odd step)
+template <int DT, bool ODD>
+__device__ __forceinline__ void stage_pair(const CaseArgs<float>& a, int c0a, int c0b, int lane, char* buf, uint64_t* bar,
+                                           int pad)
+{
+    using G = StageGeom<DT>;
+    if (lane == 0) {
+        mbar_expect_tx(bar, G::tx + (unsigned)pad);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c0 = h ? c0b : c0a;
+            char* d = buf + h * G::chunk;
+            if (!ODD) {
+                tensor_to_smem(d, &a.tm_even, c0 & ~(G::align - 1), 0, 0, bar);
+            } else {
+#pragma unroll
+                for (int lo = 0; lo < 9; ++lo)
+                    tensor_to_smem(d + lo * G::group, &a.tm_odd, group_x0(a, c0, lo) & ~(G::align - 1), lo, 0, bar);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// the shared-memory address of the value that cell c0 + j of a chunk reads for direction q:
+// slot q at the cell (even step), slot s = opp(q) at x - c_q (odd step; s = 9 hi + lo with
+// hi = 1 - cx, so the source lies hi cells into the group's window past the cell's own place)
+template <int DT, bool ODD>
+__device__ __forceinline__ const char* staged_elem(const CaseArgs<float>& a, const char* chunk_buf, int c0, int q, int j)
+{
+    using G = StageGeom<DT>;
+    if (!ODD) return chunk_buf + q * G::row + ((c0 & (G::align - 1)) + j) * G::sz;
+    const int s = 26 - q, hi = s / 9, lo = s % 9;
+    const int r = group_x0(a, c0, lo) & (G::align - 1);
+    return chunk_buf + lo * G::group + hi * G::row + (r + hi + j) * G::sz;
+}
+
+// a pair's populations from its staged windows: the raw stored value + weight of each cell,
+// or the rest state where the cell does not collide
+template <int DT, bool ODD>
+__device__ __forceinline__ void staged_pair_load(const CaseArgs<float>& a, const Chunk& ca, const Chunk& cb, bool adj, int lane,
+                                                 const char* buf, f2* f)
+{
+    using G = StageGeom<DT>;
+    const f2 isc(a.inv_scale);
+    if (adj) {
+        // lane l: cells 2l, 2l + 1 of the 64-cell span, in chunk l / 16.  Both chunks have the
+        // same window offsets (they are 32 cells apart); the even step's pairs are aligned
+        const char* cbuf = buf + (lane >> 4) * G::chunk;
+        const int j = (2 * lane) & 31;
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const char* e = staged_elem<DT, ODD>(a, cbuf, ca.c0, q, j);
+            f2 raw;
+            if constexpr (DT == 1) {
+                raw = ODD ? f2(((const float*)e)[0], ((const float*)e)[1]) : f2(*(const float2*)e);
+            } else {
+                const unsigned w = ODD ? ((unsigned)((const unsigned short*)e)[0] | ((unsigned)((const unsigned short*)e)[1] << 16))
+                                       : *(const unsigned*)e;
+                raw = Pair2<DT>::of(w);
+            }
+            const f2 w(weight<float>(q));
+            f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
+        }
+    } else {
+        const unsigned bit = 1u << lane;
+        const bool fa = (ca.fluid & bit) != 0, fb = (cb.fluid & bit) != 0;
+#pragma unroll
+        for (int q = 0; q < 27; ++q) {
+            const char* ea = staged_elem<DT, ODD>(a, buf, ca.c0, q, lane);
+            const char* eb = staged_elem<DT, ODD>(a, buf + G::chunk, cb.c0, q, lane);
+            float va, vb;
+            if constexpr (DT == 1) {
+                va = *(const float*)ea;
+                vb = *(const float*)eb;
+            } else {
+                va = Cook<DT>::of_bits(*(const unsigned short*)ea);
+                vb = Cook<DT>::of_bits(*(const unsigned short*)eb);
+            }
+            const f2 raw(fa ? va : 0.f, fb ? vb : 0.f);
+            const f2 w(weight<float>(q));
+            f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
+        }
+    }
+}
+
+template <int DT, int COL, bool ODD, int ARGS>
+__global__ void __launch_bounds__(kStagedThreads) __maxnreg__((StepRegs<DT, COL, true>::value))
+    k_step_staged(const __grid_constant__ GroupArgs<float> g)
+{
+    using G = StageGeom<DT>;
+    extern __shared__ __align__(128) char stage_smem[];
+    __shared__ __align__(8) uint64_t bars[G::warps][2];
+    // each warp's loop state between its pairs: the unit, and bits {0: this unit staged,
+    // 1: the next unit staged, 2 + b: the phase to wait for on buffer b, 4: this unit's
+    // buffer}.  It lives in shared memory across the collision, whose registers it would
+    // otherwise hold
+    __shared__ int loop_state[G::warps][2];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int step = g.cursor[ODD ? 1 : 0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) g.cursor[ODD ? 0 : 1] = step + 1;
+    const int flags = case_args<ARGS>(g, 0).ctl[step].flags;
+    uint64_t* bar = bars[wid];
+    volatile int* ls = loop_state[wid];
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    // unit u < np: the chunk pair (2u, 2u + 1); above: a batch of 32 boundary nodes
+    auto n_units = [&]() { return (g.n_chunks >> 1) + (g.n_nodes + 31) / 32; };
+    char* const smem0 = stage_smem + ((128u - (smem_addr(stage_smem) & 127u)) & 127u); // 128-byte aligned
+    auto buffer = [&](int b) { return smem0 + (wid * 2 + b) * G::unit; };
+    auto stage = [&](int u, int b) -> bool {
+        if (u >= (g.n_chunks >> 1)) return false;
+        const Chunk ca = g.chunks[2 * u], cb = g.chunks[2 * u + 1];
+        if (!pairable<ARGS>(g, ca, cb)) return false;
+        stage_pair<DT, ODD>(case_args<ARGS>(g, ca.cflags & CH_CASE_MASK), ca.c0, cb.c0, lane, buffer(b), &bar[b], g.stage_pad);
+        return true;
+    };
+    {
+        const int u = blockIdx.x * G::warps + wid;
+        const bool st = u < n_units() && stage(u, 0);
+        if (lane == 0) { ls[0] = u; ls[1] = st ? 1 : 0; }
+        __syncwarp();
+    }
+    while (true) {
+        const int u = ls[0];
+        int state = ls[1];
+        if (u >= n_units()) break;
+        const int b = (state >> 4) & 1;
+        const int un = u + gridDim.x * G::warps;
+        // the next pair's rows travel while this one collides (its buffer was released by
+        // the __syncwarp that ended the unit before)
+        if (un < n_units() && stage(un, b ^ 1)) state |= 2;
+        const int np = g.n_chunks >> 1;
+        if (u < np) {
+            const Chunk ca = g.chunks[2 * u], cb = g.chunks[2 * u + 1];
+            const int ci = ca.cflags & CH_CASE_MASK;
+            const CaseArgs<float>& a = case_args<ARGS>(g, ci);
+            if (state & 1) {
+                if (!mbar_wait(&bar[b], (state >> (2 + b)) & 1, g.stage_wait_ns)) {
+                    if (lane == 0) atomicOr(a.err, ERR_STALL);
+                    // the copies of the next pair are this warp's: let them land before it leaves
+                    if (state & 2) mbar_wait(&bar[b ^ 1], (state >> (3 - b)) & 1, g.stage_wait_ns);
+                    return;
+                }
+                state ^= 4 << b;
+                // the loop state waits in shared memory while the pair collides
+                if (lane == 0) ls[1] = state;
+                f2 f[27];
+                const bool adj = adjacent_span<DT>(ca, cb);
+                staged_pair_load<DT, ODD>(a, ca, cb, adj, lane, buffer(b), f);
+                pair_finish<DT, COL, ODD>(a, g.cases + ci, ca, cb, g.chunks + 2 * u, g.chunk_nodes + 2 * u, f, step, flags, lane,
+                                          adj);
+                __syncwarp();
+                state = ls[1];
+            } else {
+                if (lane == 0) ls[1] = state;
+                unpaired_chunks<DT, COL, ODD, ARGS>(g, u, step, flags, lane);
+                __syncwarp();
+                state = ls[1];
+            }
+        } else {
+            node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (u - np) * 32 + lane, step, flags);
+        }
+        // next: the next unit in this unit's place, its buffer the other one
+        state = ((state >> 1) & 1) | (state & (3 << 2)) | ((b ^ 1) << 4);
+        __syncwarp();
+        if (lane == 0) { ls[0] = u + gridDim.x * G::warps; ls[1] = state; }
+        __syncwarp();
     }
 }
 
@@ -1158,70 +1452,92 @@ __global__ void __launch_bounds__(256) k_output_fields(const CaseArgs<CT> a, con
 // translation unit
 // ---------------------------------------------------------------------------------------
 using GroupLauncher = void (*)(bool odd, dim3 grid, dim3 block, cudaStream_t s, const void* group_args);
+// the step kernel's launch forms: one cell a thread, two (the paired form), and the paired
+// form with staged loads (k_step_staged, persistent warps, StageGeom shared memory)
+enum : int { FORM_ONE = 0, FORM_PAIRED = 1, FORM_STAGED = 2 };
 // the step kernel's launcher: `after_gather` launches it as a programmatic dependent of the
-// gather kernel just enqueued on the stream; `paired` picks the two-cells-per-thread form
-using StepLauncher = void (*)(bool odd, bool after_gather, bool paired, dim3 grid, dim3 block, cudaStream_t s,
+// gather kernel just enqueued on the stream
+using StepLauncher = void (*)(bool odd, bool after_gather, int form, dim3 grid, dim3 block, cudaStream_t s,
                               const void* group_args);
+// resident blocks per SM of the staged form (0 where the variant has no staged form)
+using StagedOccupancy = int (*)();
 
-// launch of one step-kernel variant: one warp per chunk (per pair)
-template <int DT, int COL, bool ODD, int ARGS, bool PAIR>
+// the kernel of one step variant
+template <int DT, int COL, bool ODD, int ARGS, int FORM>
+constexpr auto step_kernel()
+{
+    if constexpr (FORM == FORM_STAGED) return &k_step_staged<DT, COL, ODD, ARGS>;
+    else return &k_step<DT, COL, ODD, ARGS, FORM == FORM_PAIRED>;
+}
+template <int DT, int FORM>
+constexpr size_t step_smem()
+{
+    if constexpr (FORM == FORM_STAGED) return (size_t)StageGeom<DT>::smem;
+    else return 0;
+}
+
+// launch of one step-kernel variant
+template <int DT, int COL, bool ODD, int ARGS, int FORM>
 void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
-    if (!after_gather) {
-        k_step<DT, COL, ODD, ARGS, PAIR><<<grid, block, 0, s>>>(g);
-        return;
-    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = step_smem<DT, FORM>();
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_step<DT, COL, ODD, ARGS, PAIR>, g);
+    cfg.numAttrs = after_gather ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, step_kernel<DT, COL, ODD, ARGS, FORM>(), g);
 }
 
-template <int DT, int COL, bool PAIR>
+template <int DT, int COL, int FORM>
 void launch_step_form(bool odd, bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
 {
     switch (args_mode(g.n_cases)) {
     case ARGS_ONE:
-        if (odd) launch_step_variant<DT, COL, true, ARGS_ONE, PAIR>(after_gather, grid, block, s, g);
-        else launch_step_variant<DT, COL, false, ARGS_ONE, PAIR>(after_gather, grid, block, s, g);
+        if (odd) launch_step_variant<DT, COL, true, ARGS_ONE, FORM>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, ARGS_ONE, FORM>(after_gather, grid, block, s, g);
         break;
     case ARGS_PARAM:
-        if (odd) launch_step_variant<DT, COL, true, ARGS_PARAM, PAIR>(after_gather, grid, block, s, g);
-        else launch_step_variant<DT, COL, false, ARGS_PARAM, PAIR>(after_gather, grid, block, s, g);
+        if (odd) launch_step_variant<DT, COL, true, ARGS_PARAM, FORM>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, ARGS_PARAM, FORM>(after_gather, grid, block, s, g);
         break;
     default:
-        if (odd) launch_step_variant<DT, COL, true, ARGS_GLOBAL, PAIR>(after_gather, grid, block, s, g);
-        else launch_step_variant<DT, COL, false, ARGS_GLOBAL, PAIR>(after_gather, grid, block, s, g);
+        if (odd) launch_step_variant<DT, COL, true, ARGS_GLOBAL, FORM>(after_gather, grid, block, s, g);
+        else launch_step_variant<DT, COL, false, ARGS_GLOBAL, FORM>(after_gather, grid, block, s, g);
     }
 }
 
-// `paired`: the two-cells-per-thread form where the collision has one (pairs_chunks)
+// `form`: FORM_PAIRED and FORM_STAGED apply where the collision pairs (pairs_chunks); the
+// others step one cell a thread
 template <int DT, int COL>
-void launch_step(bool odd, bool after_gather, bool paired, dim3 grid, dim3 block, cudaStream_t s, const void* args)
+void launch_step(bool odd, bool after_gather, int form, dim3 grid, dim3 block, cudaStream_t s, const void* args)
 {
     using CT = typename Storage<DT>::CT;
     const GroupArgs<CT>& g = *(const GroupArgs<CT>*)args;
     if constexpr (pairs_chunks(DT, COL)) {
-        if (paired) {
-            launch_step_form<DT, COL, true>(odd, after_gather, grid, block, s, g);
+        if (form == FORM_PAIRED) {
+            launch_step_form<DT, COL, FORM_PAIRED>(odd, after_gather, grid, block, s, g);
+            return;
+        }
+        if (form == FORM_STAGED) {
+            launch_step_form<DT, COL, FORM_STAGED>(odd, after_gather, grid, block, s, g);
             return;
         }
     }
-    launch_step_form<DT, COL, false>(odd, after_gather, grid, block, s, g);
+    launch_step_form<DT, COL, FORM_ONE>(odd, after_gather, grid, block, s, g);
 }
 
 StepLauncher step_launcher(int dtype, int collision);
+StagedOccupancy staged_occupancy(int dtype, int collision);
 
 // Every variant of the step kernel of a (storage, collision) resolved now.  Under CUDA's lazy
 // module loading the runtime loads a kernel's code at its first launch, which allocates device
-// memory then; a context loads its kernels when it is created instead.
+// memory then; a context loads its kernels when it is created instead.  The staged form is
+// also allowed its shared memory here.
 template <int DT, int COL, bool ODD, int ARGS>
 cudaError_t load_step_variant()
 {
@@ -1229,6 +1545,9 @@ cudaError_t load_step_variant()
     cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)k_step<DT, COL, ODD, ARGS, false>);
     if constexpr (pairs_chunks(DT, COL)) {
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void*)k_step<DT, COL, ODD, ARGS, true>);
+        const void* k = (const void*)k_step_staged<DT, COL, ODD, ARGS>;
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, StageGeom<DT>::smem);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
     }
     return e;
 }
@@ -1241,6 +1560,25 @@ cudaError_t load_step()
     for (cudaError_t x : e)
         if (x != cudaSuccess) return x;
     return cudaSuccess;
+}
+// resident blocks per SM of the staged form (the fewest over its variants), 0 without one
+template <int DT, int COL>
+int staged_blocks()
+{
+    if constexpr (pairs_chunks(DT, COL)) {
+        int best = 1 << 30;
+        const void* ks[6] = {(const void*)k_step_staged<DT, COL, false, ARGS_ONE>, (const void*)k_step_staged<DT, COL, true, ARGS_ONE>,
+                             (const void*)k_step_staged<DT, COL, false, ARGS_PARAM>, (const void*)k_step_staged<DT, COL, true, ARGS_PARAM>,
+                             (const void*)k_step_staged<DT, COL, false, ARGS_GLOBAL>, (const void*)k_step_staged<DT, COL, true, ARGS_GLOBAL>};
+        for (const void* k : ks) {
+            int n = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kStagedThreads, StageGeom<DT>::smem) != cudaSuccess) return 0;
+            best = n < best ? n : best;
+        }
+        return best;
+    } else {
+        return 0;
+    }
 }
 
 } // namespace nnlbm

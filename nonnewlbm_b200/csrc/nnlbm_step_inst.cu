@@ -14,11 +14,13 @@
 #define NNLBM_CAT(a, b, c) NNLBM_CAT2(a, b, c)
 
 namespace nnlbm {
-void NNLBM_CAT(launch_step_, NNLBM_DT, NNLBM_COL)(bool odd, bool after_gather, bool paired, dim3 grid, dim3 block,
+void NNLBM_CAT(launch_step_, NNLBM_DT, NNLBM_COL)(bool odd, bool after_gather, int form, dim3 grid, dim3 block,
                                                 cudaStream_t s, const void* args)
 {
-    launch_step<NNLBM_DT, NNLBM_COL>(odd, after_gather, paired, grid, block, s, args);
+    launch_step<NNLBM_DT, NNLBM_COL>(odd, after_gather, form, grid, block, s, args);
 }
 
 cudaError_t NNLBM_CAT(load_step_, NNLBM_DT, NNLBM_COL)() { return load_step<NNLBM_DT, NNLBM_COL>(); }
+
+int NNLBM_CAT(staged_blocks_, NNLBM_DT, NNLBM_COL)() { return staged_blocks<NNLBM_DT, NNLBM_COL>(); }
 } // namespace nnlbm

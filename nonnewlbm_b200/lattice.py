@@ -139,9 +139,18 @@ class Lattice:
         flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0)
         self._chk(capi.lib().nnlbm_autotune_flags(self.h, flags))
 
-    def set_launch(self, block: int = 256, cells_per_thread: int = 2) -> None:
-        """Fix the step kernel's launch shape instead of autotuning it."""
-        self._chk(capi.lib().nnlbm_set_launch(self.h, int(block), int(cells_per_thread)))
+    def set_launch(self, block: int = 256, cells_per_thread: int = 2, staged: bool = False) -> None:
+        """Fix the step kernel's launch shape instead of autotuning it; `staged` picks the
+        two-cell form whose warps stage their populations in shared memory (block 128)."""
+        cpt = int(cells_per_thread) | (capi.LAUNCH_STAGED if staged else 0)
+        self._chk(capi.lib().nnlbm_set_launch(self.h, int(block), cpt))
+
+    def launch(self, ic: int = 0) -> dict:
+        """The launch shape case ic steps with now: block size, cells a thread, staged."""
+        b, c = ctypes.c_int(), ctypes.c_int()
+        self._chk(capi.lib().nnlbm_get_launch(self.h, ic, ctypes.byref(b), ctypes.byref(c)))
+        return {"block": b.value, "cells_per_thread": c.value & ~capi.LAUNCH_STAGED,
+                "staged": bool(c.value & capi.LAUNCH_STAGED)}
 
     def stat_reset(self, ic: int | None = None) -> None:
         for k in self._cases(ic):
