@@ -865,22 +865,6 @@ __device__ __forceinline__ bool pairable(const GroupArgs<float>& g, const Chunk&
            case_args<ARGS>(g, ci).cy_mode != CY_REF_FD;
 }
 
-// a pair of chunks that does not collide as a pair, chunk by chunk.  Out of line, so that the
-// staged kernel's loop (the pair path) keeps a small instruction footprint and its
-// registers are allocated for the pair path alone
-template <int DT, int COL, bool ODD, int ARGS>
-__device__ __noinline__ void unpaired_chunks(const GroupArgs<float>& g, int u, int step, int flags, int lane)
-{
-    const Chunk ca = g.chunks[2 * u], cb = g.chunks[2 * u + 1];
-    const int ci = ca.cflags & CH_CASE_MASK;
-    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, ci), g.cases + ci, ca, g.chunks + 2 * u, g.chunk_nodes + 2 * u, step, flags, lane);
-    if (cb.fluid) {
-        const int cj = cb.cflags & CH_CASE_MASK;
-        fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, g.chunks + 2 * u + 1, g.chunk_nodes + 2 * u + 1, step,
-                                  flags, lane);
-    }
-}
-
 // 32 boundary nodes (open-plane nodes and GEO_INFLOW nodes, one per lane): each writes
 // the equilibrium of its gathered (rho, u) (or of its prescribed inflow) into its own
 // slots, which no other cell reads or writes within the step, and adds its plane flux
@@ -1215,8 +1199,14 @@ __global__ void __launch_bounds__(kStagedThreads) __maxnreg__((StepRegs<DT, COL,
                 __syncwarp();
                 state = ls[1];
             } else {
+                // inline like the two-cell kernel's, so that both round these chunks alike
                 if (lane == 0) ls[1] = state;
-                unpaired_chunks<DT, COL, ODD, ARGS>(g, u, step, flags, lane);
+                fluid_chunk<DT, COL, ODD>(a, g.cases + ci, ca, g.chunks + 2 * u, g.chunk_nodes + 2 * u, step, flags, lane);
+                if (cb.fluid) {
+                    const int cj = cb.cflags & CH_CASE_MASK;
+                    fluid_chunk<DT, COL, ODD>(case_args<ARGS>(g, cj), g.cases + cj, cb, g.chunks + 2 * u + 1,
+                                              g.chunk_nodes + 2 * u + 1, step, flags, lane);
+                }
                 __syncwarp();
                 state = ls[1];
             }
