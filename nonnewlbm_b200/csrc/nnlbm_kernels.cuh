@@ -555,12 +555,11 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
             refd_force<CT>(ap, c, (int)sy, (int)sz, F);
             fx = F[0]; fy = F[1]; fz = F[2];
         }
-        density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
         // one inlined collision for both viscosity models (the local Carreau-Yasuda law is
         // a runtime branch inside it)
         CT Sl[6];
         const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
-        collide<CT, COL>(f, rho, ux, uy, uz, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
+        step_cell<CT, COL>(f, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl, rho, ux, uy, uz);
         // the gather of this step reads the slots written below
         pdl_wait();
         T* ps = (T*)a.df + c;
@@ -789,10 +788,9 @@ __device__ __forceinline__ void pair_finish(const CaseArgs<float>& a, const Case
         const int cA = adj ? ca.c0 + 2 * lane : ca.c0 + lane, cB = adj ? ca.c0 + 2 * lane + 1 : cb.c0 + lane;
         const f2 fx(a.fx), fy(a.fy), fz(a.fz);
         f2 rho, ux, uy, uz;
-        density_velocity<f2>(f, fx, fy, fz, rho, ux, uy, uz);
         f2 Sl[6];
         const CYParams<float> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
-        collide<f2, COL, float>(f, rho, ux, uy, uz, fx, fy, fz, f2(a.nu), a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl);
+        step_cell<f2, COL, float>(f, fx, fy, fz, f2(a.nu), a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl, rho, ux, uy, uz);
         // the gather of this step reads the slots written below
         pdl_wait();
         const f2 sc(a.scale);

@@ -195,20 +195,57 @@ template <class CT>
 __device__ __forceinline__ CT cy_nu_from_central(CT Cxx, CT Cyy, CT Czz, CT Cxy, CT Cxz, CT Cyz, CT rho, const CYParams<CT>& p,
                                                  CT* S);
 
+// the first half of the forward z pass, which needs no velocity: per (x, y) column of
+// populations (m, z, p) at f[9 ix + 3 iy + 0..2], its sum k0 = (p + m) + z, d = p - m and
+// s = p + m, in place
+template <class CT>
+__device__ __forceinline__ void cum_columns(CT* f)
+{
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        const CT m = f[3 * c], z = f[3 * c + 1], p = f[3 * c + 2];
+        const CT sp = p + m, d = p - m;
+        f[3 * c] = sp + z;
+        f[3 * c + 1] = d;
+        f[3 * c + 2] = sp;
+    }
+}
+
+// density and velocity u = (j + F/2) / rho from the columns of cum_columns: rho sums the
+// column sums, j_z their d, j_y and j_x the column sums' differences across y and x
+template <class CT>
+__device__ __forceinline__ void cum_density_velocity(const CT* k, CT fx, CT fy, CT fz, CT& rho, CT& ux, CT& uy, CT& uz)
+{
+    auto k0 = [&](int ix, int iy) { return k[9 * ix + 3 * iy]; };
+    auto d = [&](int ix, int iy) { return k[9 * ix + 3 * iy + 1]; };
+    const CT rx0 = (k0(0, 0) + k0(0, 2)) + k0(0, 1), rx1 = (k0(1, 0) + k0(1, 2)) + k0(1, 1), rx2 = (k0(2, 0) + k0(2, 2)) + k0(2, 1);
+    rho = (rx0 + rx2) + rx1;
+    const CT ir = CT(1) / rho;
+    ux = ((rx2 - rx0) + fx * CT(0.5)) * ir;
+    uy = (((k0(0, 2) - k0(0, 0)) + (k0(2, 2) - k0(2, 0))) + (k0(1, 2) - k0(1, 0)) + fy * CT(0.5)) * ir;
+    uz = ((((d(0, 0) + d(0, 2)) + (d(2, 0) + d(2, 2))) + ((d(0, 1) + d(2, 1)) + (d(1, 0) + d(1, 2)))) + d(1, 1) + fz * CT(0.5)) * ir;
+}
+
 // `cy` non-null: the shear viscosity comes from the Carreau-Yasuda law evaluated on this
 // cell's own central second moments (k_200 ... k_011 of the forward transform); S receives
-// the strain rate
+// the strain rate.  `f`: the columns of cum_columns; the post-collision populations replace
+// them
 template <class CT, class PT = CT>
-__device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu, const CYParams<PT>* cy = nullptr,
-                                            CT* S = nullptr)
+__device__ __forceinline__ void collide_cum_columns(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu, const CYParams<PT>* cy = nullptr,
+                                                    CT* S = nullptr)
 {
-    // forward: z pass over the 9 (x,y) columns
+    // forward: the z pass's second half over the 9 (x,y) columns (fwd3 from k0, d, s)
     CT a[3][3][3];
+    const CT uzz = uz * uz, m2uz = CT(-2) * uz;
 #pragma unroll
     for (int ix = 0; ix < 3; ++ix)
 #pragma unroll
-        for (int iy = 0; iy < 3; ++iy)
-            fwd3<CT>(f[9 * ix + 3 * iy], f[9 * ix + 3 * iy + 1], f[9 * ix + 3 * iy + 2], uz, a[ix][iy][0], a[ix][iy][1], a[ix][iy][2]);
+        for (int iy = 0; iy < 3; ++iy) {
+            const CT c0 = f[9 * ix + 3 * iy], d = f[9 * ix + 3 * iy + 1], sp = f[9 * ix + 3 * iy + 2];
+            a[ix][iy][0] = c0;
+            a[ix][iy][1] = mad(-uz, c0, d);
+            a[ix][iy][2] = mad(uzz, c0, mad(m2uz, d, sp));
+        }
     // y pass
     CT b[3][3][3];
 #pragma unroll
@@ -289,6 +326,15 @@ __device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, 
                 bwd3<CT>(a[ix][iy][0], a[ix][iy][1], a[ix][iy][2], wz, f[9 * ix + 3 * iy], f[9 * ix + 3 * iy + 1],
                          f[9 * ix + 3 * iy + 2]);
     }
+}
+
+// the cumulant collision from populations f and a given density and velocity
+template <class CT, class PT = CT>
+__device__ __forceinline__ void collide_cum(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu, const CYParams<PT>* cy = nullptr,
+                                            CT* S = nullptr)
+{
+    cum_columns<CT>(f);
+    collide_cum_columns<CT, PT>(f, rho, ux, uy, uz, nu, cy, S);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -500,6 +546,24 @@ __device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT f
         constexpr bool central = COL >= COL_KBC_C1;
         constexpr int v = central ? COL - COL_KBC_C1 + 1 : COL - COL_KBC_N1 + 1;
         collide_kbc<CT, central, (v == 2 || v == 4), (v == 3 || v == 4)>(f, rho, ux, uy, uz, fx, fy, fz, nu);
+    }
+}
+
+// density, velocity (u = (j + F/2) / rho) and the collision of one cell's populations.  For
+// the cumulant the first half of the forward transform's z pass sums the populations by
+// column, and the density and momentum come from those sums instead of separate sums over
+// all 27
+template <class CT, int COL, class PT = CT>
+__device__ __forceinline__ void step_cell(CT* f, CT fx, CT fy, CT fz, CT nu, const CYParams<PT>* cy, CT* S, CT& rho, CT& ux,
+                                          CT& uy, CT& uz)
+{
+    if constexpr (COL == COL_CUM) {
+        cum_columns<CT>(f);
+        cum_density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
+        collide_cum_columns<CT, PT>(f, rho, ux, uy, uz, nu, cy, S);
+    } else {
+        density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
+        collide<CT, COL, PT>(f, rho, ux, uy, uz, fx, fy, fz, nu, cy, S);
     }
 }
 
