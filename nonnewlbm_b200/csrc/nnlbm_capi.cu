@@ -290,7 +290,6 @@ void fill_case_args(Case& c, CaseArgs<CT>& a)
     for (int q = 0; q < 27; ++q) {
         const int64_t sh = cxq(q) + cyq(q) * sy + czq(q) * sz;
         a.slot_even[q] = (const void*)(base + (uintptr_t)(q * qs * S));
-        a.slot_odd_ld[q] = (const void*)(base + (uintptr_t)((oppq(q) * qs - sh) * S));
         a.slot_odd_st[q] = (const void*)(base + (uintptr_t)((q * qs + sh) * S));
     }
     c.stage_maps = false;

@@ -115,10 +115,10 @@ struct CaseArgs {
     // per-slot base addresses of a plain chunk's accesses, each the population array of one
     // slot already offset by the cell shift of the access, so that an address is one
     // shift-and-add of the cell index: slot q (even step, loads of slot q and stores of
-    // slot opp(q)); slot opp(q) at -c_q (odd-step loads of direction q); slot q at +c_q
-    // (odd-step stores of direction q)
+    // slot opp(q)); slot q at +c_q (odd-step stores of direction q).  The odd-step load of
+    // direction q, slot opp(q) at -c_q, is the store base of opp(q) (odd_ld), so the odd
+    // step's 54 accesses use 27 base addresses, like the even step's
     const void* slot_even[27];
-    const void* slot_odd_ld[27];
     const void* slot_odd_st[27];
     // the staged form's tensor maps of the population arrays (single-precision arithmetic
     // only): dims {qstride cells, 9, 3} over slot s = 9 * hi + lo, boxes of StageGeom::win
@@ -126,6 +126,13 @@ struct CaseArgs {
     // three slots of one (cy, cz) group in the odd step)
     CUtensorMap tm_even, tm_odd;
 };
+
+// the odd-step load base of direction q: slot opp(q) shifted by -c_q = +c_opp(q)
+template <class CT>
+__device__ __forceinline__ const void* odd_ld(const CaseArgs<CT>& a, int q)
+{
+    return a.slot_odd_st[26 - q];
+}
 
 // one 32-cell row chunk of the work list: the first cell, its row, the case and flags,
 // and per lane (bit = lane) which cells collide and which of those are PERIODIC
@@ -543,7 +550,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         } else if (plain) {
             // slot opp(q) at c - c_q
 #pragma unroll
-            for (int q = 0; q < 27; ++q) f[q] = S::from(((const T*)a.slot_odd_ld[q])[c], q, a.inv_scale);
+            for (int q = 0; q < 27; ++q) f[q] = S::from(((const T*)odd_ld(a, q))[c], q, a.inv_scale);
         } else {
 #pragma unroll
             for (int q = 0; q < 27; ++q)
@@ -764,7 +771,7 @@ __device__ __forceinline__ void pair_load_adjacent(const CaseArgs<float>& a, int
     const f2 isc(a.inv_scale);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
-        const void* p = ODD ? a.slot_odd_ld[q] : a.slot_even[q];
+        const void* p = ODD ? odd_ld(a, q) : a.slot_even[q];
         const f2 raw = load_adjacent<DT, ODD>((const T*)p + c0 + 2 * lane);
         const f2 w(weight<float>(q));
         f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
@@ -847,7 +854,7 @@ __device__ __forceinline__ void pair_load(const CaseArgs<float>& a, const Chunk&
     const f2 isc(a.inv_scale);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
-        const T* p = (const T*)(ODD ? a.slot_odd_ld[q] : a.slot_even[q]);
+        const T* p = (const T*)(ODD ? odd_ld(a, q) : a.slot_even[q]);
         const f2 raw(pair_get<DT>(p + cA, fa), pair_get<DT>(p + cB, fb));
         const f2 w(weight<float>(q));
         f[q] = DT == 1 ? raw + w : mad(raw, isc, w);
