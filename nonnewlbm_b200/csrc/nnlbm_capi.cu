@@ -143,6 +143,15 @@ struct Case {
     double ivc_flux = 0, svc_flux = 0, rho_left = 1, rho_right = 1, rho_eq = 1;
     std::vector<double> sched;       // rows of {ivc_flux, svc_flux, profile_scale}
     mutable std::vector<char> ctl_dev; // copy of the leading control rows on the device (empty: unknown)
+    std::vector<char> ctl_buf;       // the rows of the current call, built on the host
+    // pinned staging of the rows for their copies to the device: a ring of kCtlSlots buffers,
+    // each reused once the copy recorded by its event has run, so that asynchronous calls can
+    // run several steps ahead of the device
+    static constexpr int kCtlSlots = 4;
+    char* h_ctl[kCtlSlots] = {};
+    size_t h_ctl_bytes[kCtlSlots] = {};
+    cudaEvent_t ctl_done[kCtlSlots] = {};
+    int ctl_slot = 0;
     int64_t parity = 0;              // steps done since the layout was last reset, mod 2
     int64_t iterations = 0;
     int64_t n_stats = 0;
@@ -559,12 +568,26 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = t
         if (flags & NNLBM_STEP_STATS)
             if ((rc = ensure_stats(ctx, c)) != NNLBM_OK) return rc;
         if ((rc = ensure_ctl(ctx, c, n)) != NNLBM_OK) return rc;
-        std::vector<char> buf;
+        std::vector<char>& buf = c.ctl_buf;
         if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n, flags);
         else fill_ctl<float>(c, buf, n, flags);
-        // rows already on the device (a constant inflow stepped call after call) are not sent again
+        // rows already on the device (a constant inflow stepped call after call) are not sent again;
+        // new ones go through a pinned staging buffer, reused once its last copy has completed
         if (buf.size() > c.ctl_dev.size() || memcmp(buf.data(), c.ctl_dev.data(), buf.size()) != 0) {
-            CK(cudaMemcpyAsync(c.d_ctl, buf.data(), buf.size(), cudaMemcpyHostToDevice, ctx->stream));
+            const int k = c.ctl_slot;
+            c.ctl_slot = (k + 1) % Case::kCtlSlots;
+            if (!c.ctl_done[k]) CK(cudaEventCreateWithFlags(&c.ctl_done[k], cudaEventDisableTiming));
+            else CK(cudaEventSynchronize(c.ctl_done[k]));
+            if (c.h_ctl_bytes[k] < buf.size()) {
+                if (c.h_ctl[k]) cudaFreeHost(c.h_ctl[k]);
+                c.h_ctl[k] = nullptr;
+                c.h_ctl_bytes[k] = 0;
+                CK(cudaMallocHost((void**)&c.h_ctl[k], std::max<size_t>(buf.size(), 4096)));
+                c.h_ctl_bytes[k] = std::max<size_t>(buf.size(), 4096);
+            }
+            memcpy(c.h_ctl[k], buf.data(), buf.size());
+            CK(cudaMemcpyAsync(c.d_ctl, c.h_ctl[k], buf.size(), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaEventRecord(c.ctl_done[k], ctx->stream));
             c.ctl_dev = buf;
         }
         if (reset && (flags & NNLBM_STEP_REDUCE)) CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
@@ -1685,6 +1708,10 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
             if (p) cudaFree(p);
     }
     for (Case& c : ctx->cases) {
+        for (int k = 0; k < Case::kCtlSlots; ++k) {
+            if (c.h_ctl[k]) cudaFreeHost(c.h_ctl[k]);
+            if (c.ctl_done[k]) cudaEventDestroy(c.ctl_done[k]);
+        }
         void* ptrs[] = {c.df_base, c.d_label, c.d_macro, c.d_stats, c.d_ctl, c.d_hw};
         for (void* p : ptrs)
             if (p) cudaFree(p);
