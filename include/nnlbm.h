@@ -269,7 +269,7 @@ int nnlbm_autotune_flags(nnlbm_ctx* ctx, int flags);
  * 128 or 256) and 1 or 2 cells a thread (2 applies to the single-precision cumulant, BGK
  * and MRT; the others step one).  2 | NNLBM_LAUNCH_STAGED selects the staged form of the
  * two-cell kernel: persistent warps that bring each pair of chunks into shared memory with
- * bulk copies while they collide the pair before (its block size is fixed at 128; results
+ * bulk copies while they collide the pair before (its block size is fixed at 128; its pairs
  * are bitwise those of the two-cell form).  Replaces --block-size (sim_tcpc.cu:118-119). */
 #define NNLBM_LAUNCH_STAGED 16
 int nnlbm_set_launch(nnlbm_ctx* ctx, int block, int cells_per_thread);

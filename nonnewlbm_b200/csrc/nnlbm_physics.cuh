@@ -9,6 +9,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace nnlbm {
 
 __host__ __device__ constexpr int cxq(int q) { return q / 9 - 1; }
@@ -226,6 +228,53 @@ __device__ __forceinline__ void cum_density_velocity(const CT* k, CT fx, CT fy, 
     uz = ((((d(0, 0) + d(0, 2)) + (d(2, 0) + d(2, 2))) + ((d(0, 1) + d(2, 1)) + (d(1, 0) + d(1, 2)))) + d(1, 1) + fz * CT(0.5)) * ir;
 }
 
+// the relaxation of the cumulant (lbm_col_cum.h:205-235 with omega2 = 1 and no anti-aliasing
+// terms) from the central moments k of total order <= 2: s receives the post-collision
+// cumulants as central moments (orders 3 and 5 zero).  `cy` non-null: the shear viscosity
+// comes from the Carreau-Yasuda law on k's second moments, S receives the strain rate
+template <class CT, class PT = CT>
+__device__ __forceinline__ void cum_relax(const CT (&k)[3][3][3], CT rho, CT nu, const CYParams<PT>* cy, CT* S, CT (&s)[3][3][3])
+{
+    const CT ir = CT(1) / rho;
+    if (cy) nu = cy_nu_from_central(k[2][0][0], k[0][2][0], k[0][0][2], k[1][1][0], k[1][0][1], k[0][1][1], rho, *cy, S);
+    const CT om = CT(1) / (CT(3) * nu + CT(0.5));
+    const CT k000 = k[0][0][0];
+    // relaxation (lbm_col_cum.h:205-235 with omega2 = 1 and no anti-aliasing terms)
+    const CT s110 = (CT(1) - om) * k[1][1][0];
+    const CT s101 = (CT(1) - om) * k[1][0][1];
+    const CT s011 = (CT(1) - om) * k[0][1][1];
+    const CT e33 = (CT(1) - om) * (k[2][0][0] - k[0][2][0]);
+    const CT e34 = (CT(1) - om) * (k[2][0][0] - k[0][0][2]);
+    const CT s200 = CT(1.0 / 3.0) * (e33 + e34 + k000);
+    const CT s020 = CT(1.0 / 3.0) * (CT(-2) * e33 + e34 + k000);
+    const CT s002 = CT(1.0 / 3.0) * (e33 - CT(2) * e34 + k000);
+    // fourth order from products (Eq 81-82); third and fifth order vanish
+    const CT s211 = (s200 * s011 + CT(2) * s101 * s110) * ir;
+    const CT s121 = (s020 * s101 + CT(2) * s110 * s011) * ir;
+    const CT s112 = (s002 * s110 + CT(2) * s011 * s101) * ir;
+    const CT s220 = (s020 * s200 + CT(2) * s110 * s110) * ir;
+    const CT s022 = (s002 * s020 + CT(2) * s011 * s011) * ir;
+    const CT s202 = (s200 * s002 + CT(2) * s101 * s101) * ir;
+    // sixth order (Eq 84 with the odd orders at zero)
+    const CT s222 = (s200 * s022 + s020 * s202 + s002 * s220 + CT(4) * (s011 * s211 + s101 * s121 + s110 * s112)) * ir
+                    - (CT(16) * s110 * s101 * s011 + CT(4) * (s101 * s101 * s020 + s011 * s011 * s200 + s110 * s110 * s002)
+                       + CT(2) * s200 * s020 * s002) * ir * ir;
+
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int l = 0; l < 3; ++l) s[i][j][l] = CT(0);
+    s[0][0][0] = k000;
+    s[1][0][0] = -k[1][0][0]; s[0][1][0] = -k[0][1][0]; s[0][0][1] = -k[0][0][1];
+    s[1][1][0] = s110; s[1][0][1] = s101; s[0][1][1] = s011;
+    s[2][0][0] = s200; s[0][2][0] = s020; s[0][0][2] = s002;
+    s[2][1][1] = s211; s[1][2][1] = s121; s[1][1][2] = s112;
+    s[2][2][0] = s220; s[0][2][2] = s022; s[2][0][2] = s202;
+    s[2][2][2] = s222;
+}
+
 // `cy` non-null: the shear viscosity comes from the Carreau-Yasuda law evaluated on this
 // cell's own central second moments (k_200 ... k_011 of the forward transform); S receives
 // the strain rate.  `f`: the columns of cum_columns; the post-collision populations replace
@@ -261,45 +310,8 @@ __device__ __forceinline__ void collide_cum_columns(CT* f, CT rho, CT ux, CT uy,
         for (int kz = 0; kz < 3; ++kz)
             if (ky + kz <= 2) fwd3<CT>(b[0][ky][kz], b[1][ky][kz], b[2][ky][kz], ux, k[0][ky][kz], k[1][ky][kz], k[2][ky][kz]);
 
-    const CT ir = CT(1) / rho;
-    if (cy) nu = cy_nu_from_central(k[2][0][0], k[0][2][0], k[0][0][2], k[1][1][0], k[1][0][1], k[0][1][1], rho, *cy, S);
-    const CT om = CT(1) / (CT(3) * nu + CT(0.5));
-    const CT k000 = k[0][0][0];
-    // relaxation (lbm_col_cum.h:205-235 with omega2 = 1 and no anti-aliasing terms)
-    const CT s110 = (CT(1) - om) * k[1][1][0];
-    const CT s101 = (CT(1) - om) * k[1][0][1];
-    const CT s011 = (CT(1) - om) * k[0][1][1];
-    const CT e33 = (CT(1) - om) * (k[2][0][0] - k[0][2][0]);
-    const CT e34 = (CT(1) - om) * (k[2][0][0] - k[0][0][2]);
-    const CT s200 = CT(1.0 / 3.0) * (e33 + e34 + k000);
-    const CT s020 = CT(1.0 / 3.0) * (CT(-2) * e33 + e34 + k000);
-    const CT s002 = CT(1.0 / 3.0) * (e33 - CT(2) * e34 + k000);
-    // fourth order from products (Eq 81-82); third and fifth order vanish
-    const CT s211 = (s200 * s011 + CT(2) * s101 * s110) * ir;
-    const CT s121 = (s020 * s101 + CT(2) * s110 * s011) * ir;
-    const CT s112 = (s002 * s110 + CT(2) * s011 * s101) * ir;
-    const CT s220 = (s020 * s200 + CT(2) * s110 * s110) * ir;
-    const CT s022 = (s002 * s020 + CT(2) * s011 * s011) * ir;
-    const CT s202 = (s200 * s002 + CT(2) * s101 * s101) * ir;
-    // sixth order (Eq 84 with the odd orders at zero)
-    const CT s222 = (s200 * s022 + s020 * s202 + s002 * s220 + CT(4) * (s011 * s211 + s101 * s121 + s110 * s112)) * ir
-                    - (CT(16) * s110 * s101 * s011 + CT(4) * (s101 * s101 * s020 + s011 * s011 * s200 + s110 * s110 * s002)
-                       + CT(2) * s200 * s020 * s002) * ir * ir;
-
     CT s[3][3][3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int l = 0; l < 3; ++l) s[i][j][l] = CT(0);
-    s[0][0][0] = k000;
-    s[1][0][0] = -k[1][0][0]; s[0][1][0] = -k[0][1][0]; s[0][0][1] = -k[0][0][1];
-    s[1][1][0] = s110; s[1][0][1] = s101; s[0][1][1] = s011;
-    s[2][0][0] = s200; s[0][2][0] = s020; s[0][0][2] = s002;
-    s[2][1][1] = s211; s[1][2][1] = s121; s[1][1][2] = s112;
-    s[2][2][0] = s220; s[0][2][2] = s022; s[2][0][2] = s202;
-    s[2][2][2] = s222;
+    cum_relax<CT, PT>(k, rho, nu, cy, S, s);
     // backward: x, y, z (G2015 Eq 88-96), each axis's coefficients made just before its pass
     {
         const Bwd<CT> wx(ux);
@@ -325,6 +337,111 @@ __device__ __forceinline__ void collide_cum_columns(CT* f, CT rho, CT ux, CT uy,
             for (int iy = 0; iy < 3; ++iy)
                 bwd3<CT>(a[ix][iy][0], a[ix][iy][1], a[ix][iy][2], wz, f[9 * ix + 3 * iy], f[9 * ix + 3 * iy + 1],
                          f[9 * ix + 3 * iy + 2]);
+    }
+}
+
+// The cumulant step of one cell in single precision with the columns of x = -1 and x = 0
+// packed into f2 (the packed FP32 pipe runs both at once): the z and y passes of both
+// transforms treat the 18 populations of those two x planes as 9 pairs, the x passes (which
+// combine the planes) and the relaxation run scalar.  The operations and their order are
+// those of cum_columns / collide_cum_columns, so the results are bitwise the same.
+#ifndef NNLBM_CUM_PACKED
+#define NNLBM_CUM_PACKED 1
+#endif
+__device__ __forceinline__ void step_cell_cum_packed(float* f, float fx, float fy, float fz, float nu, const CYParams<float>* cy,
+                                                     float* S, float& rho, float& ux, float& uy, float& uz)
+{
+    // z pass, first half: per column (iy) of the planes ix = 0, 1 (P) and ix = 2 (Q)
+    f2 c0P[3], dP[3], spP[3];
+    float c0Q[3], dQ[3], spQ[3];
+#pragma unroll
+    for (int iy = 0; iy < 3; ++iy) {
+        const f2 m(f[3 * iy], f[9 + 3 * iy]), z(f[3 * iy + 1], f[9 + 3 * iy + 1]), p(f[3 * iy + 2], f[9 + 3 * iy + 2]);
+        spP[iy] = p + m;
+        dP[iy] = p - m;
+        c0P[iy] = spP[iy] + z;
+        const float mq = f[18 + 3 * iy], zq = f[18 + 3 * iy + 1], pq = f[18 + 3 * iy + 2];
+        spQ[iy] = pq + mq;
+        dQ[iy] = pq - mq;
+        c0Q[iy] = spQ[iy] + zq;
+    }
+    {
+        float k[27];
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy) {
+            k[3 * iy] = c0P[iy].v.x; k[9 + 3 * iy] = c0P[iy].v.y; k[18 + 3 * iy] = c0Q[iy];
+            k[3 * iy + 1] = dP[iy].v.x; k[9 + 3 * iy + 1] = dP[iy].v.y; k[18 + 3 * iy + 1] = dQ[iy];
+        }
+        cum_density_velocity<float>(k, fx, fy, fz, rho, ux, uy, uz);
+    }
+    // z pass, second half
+    f2 aP[3][3];
+    float aQ[3][3];
+    {
+        const f2 nuz(-uz), uzz(uz * uz), m2uz(-2.f * uz);
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy) {
+            aP[iy][0] = c0P[iy];
+            aP[iy][1] = mad(nuz, c0P[iy], dP[iy]);
+            aP[iy][2] = mad(uzz, c0P[iy], mad(m2uz, dP[iy], spP[iy]));
+            aQ[iy][0] = c0Q[iy];
+            aQ[iy][1] = mad(-uz, c0Q[iy], dQ[iy]);
+            aQ[iy][2] = mad(uz * uz, c0Q[iy], mad(-2.f * uz, dQ[iy], spQ[iy]));
+        }
+    }
+    // y pass
+    f2 bP[3][3];
+    float bQ[3][3];
+#pragma unroll
+    for (int kz = 0; kz < 3; ++kz) {
+        fwd3<f2>(aP[0][kz], aP[1][kz], aP[2][kz], f2(uy), bP[0][kz], bP[1][kz], bP[2][kz]);
+        fwd3<float>(aQ[0][kz], aQ[1][kz], aQ[2][kz], uy, bQ[0][kz], bQ[1][kz], bQ[2][kz]);
+    }
+    // x pass (scalar), orders <= 2
+    float k[3][3][3];
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz)
+            if (ky + kz <= 2) fwd3<float>(bP[ky][kz].v.x, bP[ky][kz].v.y, bQ[ky][kz], ux, k[0][ky][kz], k[1][ky][kz], k[2][ky][kz]);
+    float s[3][3][3];
+    cum_relax<float, float>(k, rho, nu, cy, S, s);
+    // backward x (scalar): the planes ix = 0, 1 of each (ky, kz) land as one pair
+    {
+        const Bwd<float> wx(ux);
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+            for (int kz = 0; kz < 3; ++kz) {
+                float m, z, p;
+                bwd3<float>(s[0][ky][kz], s[1][ky][kz], s[2][ky][kz], wx, m, z, p);
+                bP[ky][kz] = f2(m, z);
+                bQ[ky][kz] = p;
+            }
+    }
+    // backward y
+    {
+        const Bwd<f2> wy2{f2(uy)};
+        const Bwd<float> wy(uy);
+#pragma unroll
+        for (int kz = 0; kz < 3; ++kz) {
+            bwd3<f2>(bP[0][kz], bP[1][kz], bP[2][kz], wy2, aP[0][kz], aP[1][kz], aP[2][kz]);
+            bwd3<float>(bQ[0][kz], bQ[1][kz], bQ[2][kz], wy, aQ[0][kz], aQ[1][kz], aQ[2][kz]);
+        }
+    }
+    // backward z, into the populations
+    {
+        const Bwd<f2> wz2{f2(uz)};
+        const Bwd<float> wz(uz);
+#pragma unroll
+        for (int iy = 0; iy < 3; ++iy) {
+            f2 m, z, p;
+            bwd3<f2>(aP[iy][0], aP[iy][1], aP[iy][2], wz2, m, z, p);
+            f[3 * iy] = m.v.x; f[9 + 3 * iy] = m.v.y;
+            f[3 * iy + 1] = z.v.x; f[9 + 3 * iy + 1] = z.v.y;
+            f[3 * iy + 2] = p.v.x; f[9 + 3 * iy + 2] = p.v.y;
+            bwd3<float>(aQ[iy][0], aQ[iy][1], aQ[iy][2], wz, f[18 + 3 * iy], f[18 + 3 * iy + 1], f[18 + 3 * iy + 2]);
+        }
     }
 }
 
@@ -557,7 +674,9 @@ template <class CT, int COL, class PT = CT>
 __device__ __forceinline__ void step_cell(CT* f, CT fx, CT fy, CT fz, CT nu, const CYParams<PT>* cy, CT* S, CT& rho, CT& ux,
                                           CT& uy, CT& uz)
 {
-    if constexpr (COL == COL_CUM) {
+    if constexpr (COL == COL_CUM && NNLBM_CUM_PACKED && std::is_same<CT, float>::value) {
+        step_cell_cum_packed(f, fx, fy, fz, nu, cy, S, rho, ux, uy, uz);
+    } else if constexpr (COL == COL_CUM) {
         cum_columns<CT>(f);
         cum_density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
         collide_cum_columns<CT, PT>(f, rho, ux, uy, uz, nu, cy, S);
