@@ -4,8 +4,8 @@ which computes the same packed arithmetic from the same values.  Pairs must come
 equal.  Chunks that do not pair (faces, walls next to halfway bounce-back, the
 finite-difference force) are stepped one cell a thread by both kernels; the compiler may
 contract their scalar products and sums differently in the two kernels, so FP32 populations
-are compared to 1e-5 relative (a few rounding steps after 21 steps, a misplaced population
-differs by the populations' spread).  The plain form itself is checked against the FP64
+are compared to 1e-5 relative (a few rounding steps after 21 steps; a misplaced population
+differs by the populations' spread), macro fields and sums also to 1e-7 absolute.  The plain form itself is checked against the FP64
 oracle in test_gpu_parity.py; one test here checks the staged form against the oracle
 directly.
 """
@@ -54,20 +54,21 @@ def _box(nx, dtype="f32", collision="CUM"):
     return lat
 
 
-def _close(x, y, exact):
+def _close(x, y, exact, atol=1e-9):
     if exact:
         return np.array_equal(x, y)
-    return np.allclose(x, y, rtol=1e-5, atol=1e-9)
+    return np.allclose(x, y, rtol=1e-5, atol=atol)
 
 
 def _same(a: Lattice, b: Lattice, n_cases=1, stats=False, exact=True):
     for k in range(n_cases):
         assert _close(a.export_df(k), b.export_df(k), exact), k
-        assert _close(a.macro_all(k), b.macro_all(k), exact), k
+        # velocities of order 0.05 that cross zero: 1e-7 absolute beside the relative bound
+        assert _close(a.macro_all(k), b.macro_all(k), exact, atol=1e-7), k
         if stats:
             sa, na = a.stats(k)
             sb, nb = b.stats(k)
-            assert na == nb and _close(sa, sb, exact), k
+            assert na == nb and _close(sa, sb, exact, atol=1e-7), k
 
 
 def _compare(make, n_cases=1, stats=False, steps=(1, 1, 5, 13), exact=True):
@@ -81,7 +82,7 @@ def _compare(make, n_cases=1, stats=False, steps=(1, 1, 5, 13), exact=True):
         staged.step(n, macro=True, stats=stats, reduce=True)
         _same(plain, staged, n_cases, stats, exact)
     for k in range(n_cases):
-        assert _close(plain.reduce(k), staged.reduce(k), exact)
+        assert _close(plain.reduce(k), staged.reduce(k), exact, atol=1e-7)
 
 
 @pytest.mark.parametrize("nx", [130, 131])
