@@ -447,6 +447,21 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     CK(cudaMemset(g.d_bc_buf, 0, std::max<int64_t>(self_off, 1) * 4 * sizeof(CT)));
     g.n_chunks = (int)chunks.size();
     g.n_gather = (int)gather.size();
+    // room in L2 for the work lists the step launches mark persisting (the limit is this
+    // process's; it is raised, never lowered, and capped by the device)
+    {
+        size_t want = 0;
+        for (const Group& h : ctx->groups) {
+            const size_t b = (size_t)(&h == &g ? chunks.size() : h.n_chunks) * sizeof(Chunk);
+            if (b <= kPersistChunkBytes) want += b;
+        }
+        int max_persist = 0;
+        size_t cur = 0;
+        if (want > 0 && cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device) == cudaSuccess &&
+            cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize) == cudaSuccess && cur < want && max_persist > 0)
+            cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, std::min(want, (size_t)max_persist));
+        cudaGetLastError();
+    }
     g.n_self = self_off;
     GroupArgs<CT>& ga = *(GroupArgs<CT>*)g.args.data();
     memset(&ga, 0, sizeof ga);

@@ -1471,6 +1471,13 @@ constexpr size_t step_smem()
     else return 0;
 }
 
+// the work list stays in L2 between steps where it is small (a sparse geometry's list is
+// read at the head of every warp's dependent chain; a dense box's streams once per step)
+#ifndef NNLBM_PERSIST_CHUNKS
+#define NNLBM_PERSIST_CHUNKS 1
+#endif
+constexpr size_t kPersistChunkBytes = size_t(16) << 20;
+
 // launch of one step-kernel variant
 template <int DT, int COL, bool ODD, int ARGS, int FORM>
 void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t s, const GroupArgs<typename Storage<DT>::CT>& g)
@@ -1480,11 +1487,25 @@ void launch_step_variant(bool after_gather, dim3 grid, dim3 block, cudaStream_t 
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = step_smem<DT, FORM>();
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchAttribute attr[2];
+    int n = 0;
+    if (after_gather) {
+        attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n].val.programmaticStreamSerializationAllowed = 1;
+        ++n;
+    }
+    const size_t chunk_bytes = (size_t)g.n_chunks * sizeof(Chunk);
+    if (NNLBM_PERSIST_CHUNKS && chunk_bytes > 0 && chunk_bytes <= kPersistChunkBytes) {
+        attr[n].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[n].val.accessPolicyWindow.base_ptr = (void*)g.chunks;
+        attr[n].val.accessPolicyWindow.num_bytes = chunk_bytes;
+        attr[n].val.accessPolicyWindow.hitRatio = 1.0f;
+        attr[n].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[n].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        ++n;
+    }
     cfg.attrs = attr;
-    cfg.numAttrs = after_gather ? 1 : 0;
+    cfg.numAttrs = n;
     cudaLaunchKernelEx(&cfg, step_kernel<DT, COL, ODD, ARGS, FORM>(), g);
 }
 
