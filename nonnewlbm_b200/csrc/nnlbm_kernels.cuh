@@ -500,12 +500,22 @@ __host__ __device__ constexpr bool pairs_chunks(int dt, int col)
 #ifndef NNLBM_CHUNK_REGS_F32
 #define NNLBM_CHUNK_REGS_F32 80
 #endif
+// the one-cell cumulant runs packed columns (step_cell_cum_packed) with every
+// single-precision storage type; with FP16/BF16 storage it gets NNLBM_CHUNK_REGS_CUM16
+// registers (72: the packed pairs spill at 64, and 128-thread blocks keep 28 warps per SM)
+#ifndef NNLBM_PACK_DT
+#define NNLBM_PACK_DT(dt) ((dt) != 0)
+#endif
+#ifndef NNLBM_CHUNK_REGS_CUM16
+#define NNLBM_CHUNK_REGS_CUM16 72
+#endif
 template <int DT, int COL, bool PAIR>
 struct StepRegs {
     static constexpr int value = DT == 0                ? 255
                                  : !pairs_chunks(DT, COL) ? 128
                                  : PAIR                   ? NNLBM_PAIR_REGS
                                  : DT == 1                ? NNLBM_CHUNK_REGS_F32
+                                 : COL == COL_CUM         ? NNLBM_CHUNK_REGS_CUM16
                                                           : NNLBM_CHUNK_REGS;
 };
 
@@ -566,7 +576,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         // a runtime branch inside it)
         CT Sl[6];
         const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
-        step_cell<CT, COL, CT, DT == 1>(f, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl, rho, ux, uy, uz);
+        step_cell<CT, COL, CT, NNLBM_PACK_DT(DT)>(f, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl, rho, ux, uy, uz);
         // the gather of this step reads the slots written below
         pdl_wait();
         T* ps = (T*)a.df + c;

@@ -670,9 +670,7 @@ __device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT f
 // the cumulant the first half of the forward transform's z pass sums the populations by
 // column, and the density and momentum come from those sums instead of separate sums over
 // all 27
-// PACK: the one-cell cumulant in single precision uses step_cell_cum_packed (the FP32-storage
-// step; with 16-bit storage at its 64-register budget the packed pairs spill more than they
-// save)
+// PACK: the one-cell cumulant in single precision uses step_cell_cum_packed
 template <class CT, int COL, class PT = CT, bool PACK = false>
 __device__ __forceinline__ void step_cell(CT* f, CT fx, CT fy, CT fz, CT nu, const CYParams<PT>* cy, CT* S, CT& rho, CT& ux,
                                           CT& uy, CT& uz)
