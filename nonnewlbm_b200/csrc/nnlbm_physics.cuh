@@ -623,11 +623,15 @@ __device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, 
     }
     const FactEq<CT> E(ux, uy, uz);
     const CT beta = CT(1) / (CT(2) * nu / cs2 + CT(1));
+    // the shear part is linear in the moments: Delta s_q = s_q(m) - s_q(m_eq) = s_q(m - m_eq)
+    const KbcMom<CT> dm = {m.T - e.T, m.Nxz - e.Nxz, m.Nyz - e.Nyz, m.Pxy - e.Pxy, m.Pxz - e.Pxz, m.Pyz - e.Pyz,
+                           m.Qxxy - e.Qxxy, m.Qxxz - e.Qxxz, m.Qxyy - e.Qxyy, m.Qyyz - e.Qyyz, m.Qxzz - e.Qxzz,
+                           m.Qyzz - e.Qyzz, m.Qxyz - e.Qxyz};
     CT num = CT(0), den = CT(0);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const CT feq = E(q, rho);
-        const CT ds = kbc_shear<CT, USE_T, USE_Q>(q, m) - kbc_shear<CT, USE_T, USE_Q>(q, e);
+        const CT ds = kbc_shear<CT, USE_T, USE_Q>(q, dm);
         const CT dh = f[q] - feq - ds;
         const CT ifeq = CT(1) / feq;
         num += ds * dh * ifeq;
@@ -638,7 +642,7 @@ __device__ __forceinline__ void collide_kbc(CT* f, CT rho, CT ux, CT uy, CT uz, 
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const CT feq = E(q, rho);
-        const CT ds = kbc_shear<CT, USE_T, USE_Q>(q, m) - kbc_shear<CT, USE_T, USE_Q>(q, e);
+        const CT ds = kbc_shear<CT, USE_T, USE_Q>(q, dm);
         const CT dh = f[q] - feq - ds;
         f[q] -= beta * (CT(2) * ds + gamma * dh) - (CT(1) - beta) * force_src<CT>(q, ir, ux, uy, uz, fx, fy, fz) * feq;
     }
