@@ -436,12 +436,12 @@ def dense_box_lines(dev: int, warmup: int, steps: int, shape=(768, 576, 480), va
     return out
 
 
-def batch_gain(dev: int) -> dict:
+def batch_gain(dev: int, dtype: str = "f32") -> dict:
     """The 15-case study (5 inflow pairs x 3 rheologies, seeded scales in [0.5, 1]): one
     batched launch group against the cases stepped one after another."""
     from nonnewlbm_b200 import studies
 
-    r = studies.run_batch(studies.batch_cases(seed=2024, dtype="f32"), steps=100, warmup=10, device=dev)
+    r = studies.run_batch(studies.batch_cases(seed=2024, dtype=dtype), steps=100, warmup=10, device=dev)
     return {k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items() if k != "scales"}
 
 
@@ -534,6 +534,7 @@ def run_ours(a, dist: Dist) -> int:
                 line["storage_f16"] = storage_comparison(a, flush, dev, value)
                 if a.workload == "junction":
                     line["batch"] = batch_gain(dev)
+                    line["batch_f16"] = batch_gain(dev, "f16")
                     line["dense_box"] = dense_box_lines(dev, a.dense_warmup, a.dense_steps)
         line["reduce_last"] = [float(v) for v in red] if red is not None else None
         print(json.dumps(line))
