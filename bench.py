@@ -488,7 +488,8 @@ def run_ours(a, dist: Dist) -> int:
 
     # end to end through the public API: per step the host sends that step's inflow row
     # (a +-1 % pulsation, so every row differs from the last and is uploaded) and reads
-    # back the FP64 mass / flux sums
+    # back the step's status block with its FP64 mass / flux sums (NNLBM_STEP_READBACK),
+    # one step deep: step k + 1 is enqueued before the host waits for the sums of step k
     if w.kind == "tcpc":
         q0 = np.array([w.u_ivc * w.notes["counts"]["left_area"], w.u_svc * w.notes["counts"]["right_area"]])
     else:
@@ -499,8 +500,10 @@ def run_ours(a, dist: Dist) -> int:
     red = None
     for k in range(a.e2e_steps):
         lat.set_schedule(rows[k])
-        lat.step(1, stats=stats, reduce=True)
-        red = lat.reduce()
+        lat.step(1, stats=stats, reduce=True, wait=False, readback=True)
+        if k > 0:
+            red = lat.readback()[0]
+    red = lat.readback()[0]
     t_e2e = time.perf_counter() - t0
     t_e2e = dist.max(t_e2e)
     e2e = fluid * a.e2e_steps * dist.world / t_e2e / 1e6

@@ -91,9 +91,14 @@ enum {
     NNLBM_STEP_STATS = 1, /* accumulate the mean/rms sums (MacroTcpc::outputMacro, sim_tcpc.cu:347-353) */
     NNLBM_STEP_MACRO = 2, /* store rho, u, F and S of every cell */
     NNLBM_STEP_REDUCE = 4, /* FP64 mass and plane-flux sums (nnlbm_reduce) */
-    NNLBM_STEP_ASYNC = 8   /* enqueue the steps and return without waiting; the watchdog is
+    NNLBM_STEP_ASYNC = 8,  /* enqueue the steps and return without waiting; the watchdog is
                               checked by the next nnlbm_sync or synchronous nnlbm_step */
+    NNLBM_STEP_READBACK = 16 /* with NNLBM_STEP_ASYNC only: after the steps, also enqueue a copy of
+                              the context's status block (step cursors, watchdog flags, the FP64
+                              sums of NNLBM_STEP_REDUCE) into the next of NNLBM_READBACK_SLOTS
+                              pinned host slots, for nnlbm_readback */
 };
+#define NNLBM_READBACK_SLOTS 4
 
 /* One lattice (case).  Physical inputs are already in lattice units; the unit conversions
  * of sim_tcpc.cu:795-814 live in the Python host layer. */
@@ -295,6 +300,16 @@ int nnlbm_profile_step(nnlbm_ctx* ctx, int ic, int64_t n_steps, int flags, doubl
  * loop synchronises the device after every SimUpdate (core.h:1197-1198, 1256-1257); with
  * NNLBM_STEP_ASYNC the caller chooses when. */
 int nnlbm_sync(nnlbm_ctx* ctx);
+
+/* Wait for the oldest status copy enqueued by NNLBM_STEP_READBACK, check its step cursors and
+ * watchdog flags as nnlbm_sync does, and return its FP64 sums in the layout of nnlbm_reduce, 5
+ * doubles per case in case order (`out` holds n_cases >= the context's cases).  Copies are
+ * returned in the order the calls enqueued them; NNLBM_ERR_ARG when none is pending, and
+ * nnlbm_step refuses NNLBM_STEP_READBACK while NNLBM_READBACK_SLOTS copies are pending.  A loop
+ * that enqueues step k + 1 before it reads the sums of step k keeps the device busy while the
+ * host waits for each copy.  No reference counterpart (the reference synchronises after every
+ * step, core.h:1197-1198). */
+int nnlbm_readback(nnlbm_ctx* ctx, double* out, int n_cases);
 
 /* Raw CUDA stream (cudaStream_t) of the context, for callers that interleave their own work. */
 void* nnlbm_stream(nnlbm_ctx* ctx);

@@ -21,7 +21,8 @@ EQ_INV_CUM_REF, EQ_INV_CUM, EQ_DEFAULT, EQ_ENTROPIC = 0, 1, 2, 3
 EQUILIBRIA = {"inv_cum_ref": 0, "inv_cum": 1, "default": 2, "entropic": 3}
 CY_NONE, CY_REF_FD, CY_LOCAL_NEQ = 0, 1, 2
 CY_MODES = {"none": 0, "ref-fd": 1, "ref_fd": 1, "local-neq": 2, "local_neq": 2}
-STEP_STATS, STEP_MACRO, STEP_REDUCE, STEP_ASYNC = 1, 2, 4, 8
+STEP_STATS, STEP_MACRO, STEP_REDUCE, STEP_ASYNC, STEP_READBACK = 1, 2, 4, 8, 16
+READBACK_SLOTS = 4
 LAUNCH_STAGED = 16  # OR into cells_per_thread: the staged two-cell form
 M_RHO, M_VX, M_VY, M_VZ, M_FX, M_FY, M_FZ, M_S11, M_S12, M_S13, M_S22, M_S32, M_S33 = range(13)
 M_N = 13
@@ -29,7 +30,7 @@ M_N = 13
 EXPORTED = [
     "nnlbm_create", "nnlbm_set_map", "nnlbm_setup_tcpc", "nnlbm_init_equilibrium", "nnlbm_set_inflow",
     "nnlbm_set_inflow_profile", "nnlbm_set_schedule", "nnlbm_step", "nnlbm_step_noalloc", "nnlbm_stat_reset", "nnlbm_get_macro",
-    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_import_stats", "nnlbm_import_macro", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_set_launch", "nnlbm_get_launch", "nnlbm_step_info", "nnlbm_profile_step",
+    "nnlbm_get_stats", "nnlbm_export_df", "nnlbm_import_df", "nnlbm_import_stats", "nnlbm_import_macro", "nnlbm_reduce", "nnlbm_autotune", "nnlbm_autotune_flags", "nnlbm_set_launch", "nnlbm_get_launch", "nnlbm_readback", "nnlbm_step_info", "nnlbm_profile_step",
     "nnlbm_stream", "nnlbm_last_error", "nnlbm_destroy", "nnlbm_tcpc_labels", "nnlbm_sync", "nnlbm_output_fields",
 ]
 # the VTK output fields of nnlbm_output_fields, in file order, with their components
@@ -92,6 +93,7 @@ def lib():
         L.nnlbm_autotune_flags.argtypes = [_vp, i]
         L.nnlbm_set_launch.argtypes = [_vp, i, i]
         L.nnlbm_get_launch.argtypes = [_vp, i, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.nnlbm_readback.argtypes = [_vp, _dp, i]
         L.nnlbm_step_info.argtypes = [_vp, i, _i64p, _i64p, _i64p, _dp]
         L.nnlbm_profile_step.argtypes = [_vp, i, ctypes.c_int64, i, _dp, _i64p]
         L.nnlbm_sync.argtypes = [_vp]

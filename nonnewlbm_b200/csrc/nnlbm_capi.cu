@@ -209,6 +209,17 @@ struct nnlbm_ctx {
     char* h_status = nullptr;        // its pinned host mirror
     bool status_fresh = false;       // the mirror holds the block as the last step left it
     int sm_count = 0;
+    // copies of the status block enqueued by NNLBM_STEP_READBACK, oldest first: pinned slots,
+    // the event after each copy, and what its check needs (the steps of the call, each group's
+    // A-A parity after them)
+    struct Readback {
+        char* h = nullptr;
+        cudaEvent_t done = nullptr;
+        int64_t n = 0;
+        std::vector<int> parity;
+    };
+    Readback rb[NNLBM_READBACK_SLOTS];
+    int rb_head = 0, rb_count = 0;
     // the staged step's bounded waits (GroupArgs::stage_wait_ns, stage_pad)
     long long stage_wait_ns = 2000000000LL;
     int stage_pad = 0;
@@ -647,10 +658,11 @@ int read_status(nnlbm_ctx* ctx)
     return NNLBM_OK;
 }
 
-int check_watchdog(nnlbm_ctx* ctx)
+// the watchdog flags of a status block copy (the host mirror by default)
+int check_watchdog(nnlbm_ctx* ctx, const char* status = nullptr)
 {
     const StatusLayout sl(ctx->cases.size());
-    const int* err = (const int*)(ctx->h_status + sl.err);
+    const int* err = (const int*)((status ? status : ctx->h_status) + sl.err);
     for (size_t i = 0; i < ctx->cases.size(); ++i)
         if (err[2 * i] & ERR_STALL)
             return set_err(ctx, NNLBM_ERR_TIMEOUT, "case %zu: a staged step waited %.3f s for its bulk copies and gave up", i,
@@ -660,17 +672,31 @@ int check_watchdog(nnlbm_ctx* ctx)
     return NNLBM_OK;
 }
 
+// the step cursors of a status block copy after n steps that left group i at parity[i]
+int check_cursors(nnlbm_ctx* ctx, const char* status, int64_t n, const std::vector<int>& parity)
+{
+    const int* cur = (const int*)(status + StatusLayout(ctx->cases.size()).cur);
+    for (size_t i = 0; i < ctx->groups.size(); ++i) {
+        // the last step stored n into the cursor of the parity the group is at now
+        const int k = 4 * (int)i + (parity[i] & 1);
+        if (cur[k] != n)
+            return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", i, cur[k], (long long)n);
+    }
+    return NNLBM_OK;
+}
+
+std::vector<int> group_parities(const nnlbm_ctx* ctx)
+{
+    std::vector<int> p;
+    for (const Group& g : ctx->groups) p.push_back((int)(ctx->cases[g.cases[0]].parity & 1));
+    return p;
+}
+
 int wait_and_check(nnlbm_ctx* ctx, int64_t n)
 {
     int rc = read_status(ctx);
     if (rc != NNLBM_OK) return rc;
-    const int* cur = (const int*)(ctx->h_status + StatusLayout(ctx->cases.size()).cur);
-    for (size_t i = 0; i < ctx->groups.size(); ++i) {
-        // the last step stored n into the cursor of the parity the group is at now
-        const int k = 4 * (int)i + (int)(ctx->cases[ctx->groups[i].cases[0]].parity & 1);
-        if (cur[k] != n)
-            return set_err(ctx, NNLBM_ERR_CUDA, "launch group %zu: step cursor %d after %lld steps", i, cur[k], (long long)n);
-    }
+    if ((rc = check_cursors(ctx, ctx->h_status, n, group_parities(ctx))) != NNLBM_OK) return rc;
     return check_watchdog(ctx);
 }
 
@@ -1176,6 +1202,10 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
     if (!ctx) return NNLBM_ERR_ARG;
     if (n_steps < 0) return set_err(ctx, NNLBM_ERR_ARG, "negative step count");
     if (n_steps == 0) return NNLBM_OK;
+    if ((flags & NNLBM_STEP_READBACK) && !(flags & NNLBM_STEP_ASYNC))
+        return set_err(ctx, NNLBM_ERR_ARG, "NNLBM_STEP_READBACK needs NNLBM_STEP_ASYNC");
+    if ((flags & NNLBM_STEP_READBACK) && ctx->rb_count == NNLBM_READBACK_SLOTS)
+        return set_err(ctx, NNLBM_ERR_ARG, "%d status copies pending: call nnlbm_readback first", NNLBM_READBACK_SLOTS);
     CK(cudaSetDevice(ctx->device));
     // one memset restarts every group's step cursors (and, for a reduction, every case's sums)
     const StatusLayout sl(ctx->cases.size());
@@ -1191,8 +1221,46 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         if (n_steps < rows) c.sched.erase(c.sched.begin(), c.sched.begin() + 3 * n_steps);
         else c.sched.erase(c.sched.begin(), c.sched.end() - 3);
     }
+    if (flags & NNLBM_STEP_READBACK) {
+        nnlbm_ctx::Readback& r = ctx->rb[(ctx->rb_head + ctx->rb_count) % NNLBM_READBACK_SLOTS];
+        if (!r.h) {
+            CK(cudaMallocHost((void**)&r.h, sl.bytes));
+            CK(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+        }
+        CK(cudaMemcpyAsync(r.h, ctx->d_status, sl.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaEventRecord(r.done, ctx->stream));
+        r.n = n_steps;
+        r.parity = group_parities(ctx);
+        ctx->rb_count++;
+    }
     if (flags & NNLBM_STEP_ASYNC) return NNLBM_OK;
     return wait_and_check(ctx, n_steps);
+}
+
+int nnlbm_readback(nnlbm_ctx* ctx, double* out, int n_cases)
+{
+    if (!ctx) return NNLBM_ERR_ARG;
+    if (!out || n_cases < (int)ctx->cases.size())
+        return set_err(ctx, NNLBM_ERR_ARG, "the output holds %d cases, the context has %zu", n_cases, ctx->cases.size());
+    if (ctx->rb_count == 0) return set_err(ctx, NNLBM_ERR_ARG, "no status copy pending (NNLBM_STEP_READBACK)");
+    CK(cudaSetDevice(ctx->device));
+    nnlbm_ctx::Readback& r = ctx->rb[ctx->rb_head];
+    ctx->rb_head = (ctx->rb_head + 1) % NNLBM_READBACK_SLOTS;
+    ctx->rb_count--;
+    CK(cudaEventSynchronize(r.done));
+    int rc = check_cursors(ctx, r.h, r.n, r.parity);
+    if (rc == NNLBM_OK) rc = check_watchdog(ctx, r.h);
+    if (rc != NNLBM_OK) return rc;
+    const StatusLayout sl(ctx->cases.size());
+    for (size_t ic = 0; ic < ctx->cases.size(); ++ic) {
+        const double* red = (const double*)(r.h + sl.red + kRedBytes * ic);
+        for (int k = 0; k < 5; ++k) {
+            double v = 0.0;
+            for (int i = 0; i < kRedStripes; ++i) v += red[8 * i + k];
+            out[5 * ic + k] = v;
+        }
+    }
+    return NNLBM_OK;
 }
 
 int nnlbm_sync(nnlbm_ctx* ctx)
@@ -1730,6 +1798,10 @@ int nnlbm_destroy(nnlbm_ctx* ctx)
         void* ptrs[] = {c.df_base, c.d_label, c.d_macro, c.d_stats, c.d_ctl, c.d_hw};
         for (void* p : ptrs)
             if (p) cudaFree(p);
+    }
+    for (auto& r : ctx->rb) {
+        if (r.h) cudaFreeHost(r.h);
+        if (r.done) cudaEventDestroy(r.done);
     }
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);

@@ -117,12 +117,16 @@ class Lattice:
         self._chk(capi.lib().nnlbm_set_schedule(self.h, ic, capi.dptr(a), a.shape[0]))
 
     # -- time stepping --------------------------------------------------------------------
-    def step(self, n: int = 1, stats: bool = False, macro: bool = False, reduce: bool = False, wait: bool = True) -> None:
+    def step(self, n: int = 1, stats: bool = False, macro: bool = False, reduce: bool = False, wait: bool = True,
+             readback: bool = False) -> None:
         """Advance n steps.  wait=False enqueues them and returns at once (NNLBM_STEP_ASYNC);
-        sync() then waits and checks the watchdog."""
+        sync() then waits and checks the watchdog.  readback=True (with wait=False) also
+        enqueues a copy of the step cursors, watchdog flags and FP64 sums for readback()."""
         flags = (capi.STEP_STATS if stats else 0) | (capi.STEP_MACRO if macro else 0) | (capi.STEP_REDUCE if reduce else 0)
         if not wait:
             flags |= capi.STEP_ASYNC
+        if readback:
+            flags |= capi.STEP_READBACK
         self._chk(capi.lib().nnlbm_step(self.h, int(n), flags))
 
     def sync(self) -> None:
@@ -216,6 +220,13 @@ class Lattice:
             fields.append((name, a))
             k += dofs
         return fields
+
+    def readback(self) -> np.ndarray:
+        """The oldest copy enqueued by step(readback=True), checked like sync(): [case][5] FP64
+        sums in the layout of reduce()."""
+        out = np.zeros((len(self.specs), 5))
+        self._chk(capi.lib().nnlbm_readback(self.h, capi.dptr(out), len(self.specs)))
+        return out
 
     def reduce(self, ic: int = 0) -> np.ndarray:
         out = np.zeros(5)

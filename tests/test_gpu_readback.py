@@ -1,0 +1,77 @@
+"""Pipelined stepping with NNLBM_STEP_READBACK: every step's control row goes to the device and its
+status block (step cursors, watchdog flags, FP64 sums) comes back, with the next step enqueued
+before the host waits for the copy.  The sums and the populations must be bitwise those of the
+same steps taken synchronously one by one."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from nonnewlbm_b200 import CaseSpec, Lattice, capi
+
+from helpers import small_junction
+
+pytestmark = pytest.mark.gpu
+
+
+def _lattice(n_cases=1):
+    wall = small_junction()
+    nz, ny, nx = wall.shape
+    lat = Lattice([CaseSpec((nx, ny, nz), dtype="f32", nu=0.02 * (1 + 0.5 * k)) for k in range(n_cases)])
+    areas = []
+    for k in range(n_cases):
+        c = lat.setup_tcpc(wall, ic=k)
+        areas.append((c["left_area"], c["right_area"]))
+    lat.init_equilibrium()
+    return lat, areas
+
+
+def _row(areas, k, step):
+    a, b = areas[k]
+    s = 1.0 + 0.05 * np.sin(0.3 * step + k)
+    return np.array([[0.03 * a * s, 0.02 * b * s, 1.0]])
+
+
+@pytest.mark.parametrize("n_cases", [1, 3])
+def test_pipelined_readback_matches_synchronous_steps(n_cases):
+    n = 12
+    sync, areas = _lattice(n_cases)
+    pipe, _ = _lattice(n_cases)
+    expect = []
+    for step in range(n):
+        for k in range(n_cases):
+            sync.set_schedule(_row(areas, k, step), ic=k)
+        sync.step(1, stats=True, reduce=True)
+        expect.append(np.array([sync.reduce(k) for k in range(n_cases)]))
+    got = []
+    for step in range(n):
+        for k in range(n_cases):
+            pipe.set_schedule(_row(areas, k, step), ic=k)
+        pipe.step(1, stats=True, reduce=True, wait=False, readback=True)
+        if step > 0:
+            got.append(pipe.readback())  # the step before this one
+    got.append(pipe.readback())
+    assert len(got) == n
+    for e, g in zip(expect, got):
+        assert np.array_equal(e, g)
+    for k in range(n_cases):
+        assert np.array_equal(sync.export_df(k), pipe.export_df(k))
+        assert np.array_equal(sync.stats(k)[0], pipe.stats(k)[0])
+
+
+def test_readback_refusals():
+    lat, _ = _lattice()
+    with pytest.raises(capi.NnlbmError):
+        lat.readback()  # nothing pending
+    with pytest.raises(capi.NnlbmError):
+        lat.step(1, reduce=True, readback=True)  # needs NNLBM_STEP_ASYNC
+    for _ in range(capi.READBACK_SLOTS):
+        lat.step(1, reduce=True, wait=False, readback=True)
+    with pytest.raises(capi.NnlbmError):
+        lat.step(1, reduce=True, wait=False, readback=True)  # every slot pending
+    for _ in range(capi.READBACK_SLOTS):
+        assert lat.readback().shape == (1, 5)
+    with pytest.raises(capi.NnlbmError):
+        lat.readback()
+    lat.step(2, reduce=True)  # synchronous steps go on as before
+    assert np.isfinite(lat.reduce()).all()
