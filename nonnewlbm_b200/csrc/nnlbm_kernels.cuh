@@ -14,18 +14,23 @@
 // solver/sim_tcpc/sim_tcpc.cu:235-241) need no work at all under A-A: their post-step
 // value f*_q = incoming f_opp(q) already sits in the slot the neighbour reads next.
 //
-// Work decomposition: a packed list of 32-cell row chunks of colliding cells (one warp
-// each, or one warp per two chunks in single-precision arithmetic), over all cases of
-// a launch group (same storage type and collision), followed by warps of 32 boundary
-// nodes.  Per-case parameters live in a device array indexed by the chunk's case, and in
-// parameter space for groups of up to 16 cases (case_args).
+// Work decomposition: a packed list of 32-cell row chunks of colliding cells over all
+// cases of a launch group (same storage type and collision), followed by warps of 32
+// boundary nodes.  Three launch forms, picked by the host's autotuner: one warp per chunk
+// (one cell a thread), one warp per two chunks (two cells a thread on the packed FP32 pipe,
+// single-precision arithmetic only), and the staged form of the latter (persistent warps
+// that bring their next pair into shared memory with tensor copies).  Per-case parameters
+// live in a device array indexed by the chunk's case, and in parameter space for groups of
+// up to 16 cases (case_args).
 //
 // Open-plane nodes (TCPC IVC/SVC inflow and outlets, generic GEO_OUTFLOW_RIGHT_EQ) pull a
-// stencil re-centred one cell inward (sim_tcpc.cu:242-273, lbm_bc.h:147-152).  k_bc_gather
-// computes their density / velocity from the pre-step state before the step kernel runs;
-// the node warps of the step kernel then write each node's equilibrium into the node's
-// own slots, which no other cell touches within the step.  GEO_INFLOW nodes take their
-// prescribed velocity and need no gather.
+// stencil re-centred one cell inward (sim_tcpc.cu:242-273, lbm_bc.h:147-152).  Where that
+// inward cell collides and lies off every face, the stencil is the cell's own pull, so the
+// cell's thread writes the node's equilibrium into the node's slots (serve_nodes).  For the
+// other nodes k_bc_gather computes density / velocity from the pre-step state before the
+// step kernel runs, and the node warps of the step kernel write each node's equilibrium
+// into the node's own slots, which no other cell touches within the step.  GEO_INFLOW
+// nodes take their prescribed velocity and need no gather.
 #pragma once
 
 #include <cuda.h>
