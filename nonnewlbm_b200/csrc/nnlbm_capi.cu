@@ -220,8 +220,6 @@ struct nnlbm_ctx {
     };
     Readback rb[NNLBM_READBACK_SLOTS];
     int rb_head = 0, rb_count = 0;
-    char* rb_dev[NNLBM_READBACK_SLOTS] = {}; // the slots' device-side addresses (mapped pinned memory)
-    int publish_slot = -1;                   // the slot the current call's last step publishes into
     // the staged step's bounded waits (GroupArgs::stage_wait_ns, stage_pad)
     long long stage_wait_ns = 2000000000LL;
     int stage_pad = 0;
@@ -372,9 +370,8 @@ int ensure_ctl(nnlbm_ctx* ctx, Case& c, int64_t n)
     return NNLBM_OK;
 }
 
-// publish_slot >= 0: the last step publishes the status block into that readback slot
 template <class CT>
-void fill_ctl(const Case& c, std::vector<char>& buf, int64_t n, int flags, int publish_slot = -1)
+void fill_ctl(const Case& c, std::vector<char>& buf, int64_t n, int flags)
 {
     buf.resize(n * sizeof(StepCtl<CT>));
     StepCtl<CT>* r = (StepCtl<CT>*)buf.data();
@@ -387,9 +384,8 @@ void fill_ctl(const Case& c, std::vector<char>& buf, int64_t n, int flags, int p
         }
         int f = flags & NNLBM_STEP_STATS;
         if (k == n - 1) f |= flags & (NNLBM_STEP_MACRO | NNLBM_STEP_REDUCE);
-        if (k == n - 1 && publish_slot >= 0) f |= F_PUBLISH;
         r[k].flags = f;
-        r[k].pad = k == n - 1 && publish_slot >= 0 ? publish_slot : 0;
+        r[k].pad = 0;
         // LBM_Data_Tcpc::inflowCondition{Left,Right} (sim_tcpc.cu:295-309) with
         // inflow_right = -svc_flux (sim_tcpc.cu:660), divided in the arithmetic type
         r[k].u_left = c.left_area > 0 ? (CT)ivc / (CT)c.left_area : CT(0);
@@ -495,8 +491,6 @@ int upload_group(nnlbm_ctx* ctx, Group& g)
     ga.cursor = g.d_ints;
     ga.stage_wait_ns = ctx->stage_wait_ns;
     ga.stage_pad = ctx->stage_pad;
-    ga.status_base = ctx->d_status;
-    for (int k = 0; k < NNLBM_READBACK_SLOTS; ++k) ga.rb_slots[k] = ctx->rb_dev[k];
     g.dirty = false;
     g.gen++;
     return NNLBM_OK;
@@ -601,8 +595,8 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = t
             if ((rc = ensure_stats(ctx, c)) != NNLBM_OK) return rc;
         if ((rc = ensure_ctl(ctx, c, n)) != NNLBM_OK) return rc;
         std::vector<char>& buf = c.ctl_buf;
-        if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n, flags, ctx->publish_slot);
-        else fill_ctl<float>(c, buf, n, flags, ctx->publish_slot);
+        if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n, flags);
+        else fill_ctl<float>(c, buf, n, flags);
         // rows already on the device (a constant inflow stepped call after call) are not sent again;
         // new ones go through a pinned staging buffer, reused once its last copy has completed
         if (buf.size() > c.ctl_dev.size() || memcmp(buf.data(), c.ctl_dev.data(), buf.size()) != 0) {
@@ -851,15 +845,6 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
     ctx->cases.resize(n_cases);
     // a group per case at most
     const StatusLayout sl((size_t)n_cases);
-    for (int k = 0; k < NNLBM_READBACK_SLOTS; ++k) {
-        nnlbm_ctx::Readback& r = ctx->rb[k];
-        if (cudaHostAlloc((void**)&r.h, sl.bytes, cudaHostAllocMapped) != cudaSuccess ||
-            cudaHostGetDevicePointer((void**)&ctx->rb_dev[k], r.h, 0) != cudaSuccess ||
-            cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming) != cudaSuccess) {
-            cudaGetLastError();
-            return set_err(ctx, NNLBM_ERR_OOM, "allocation of the status readback slots failed");
-        }
-    }
     if (cudaMalloc(&ctx->d_status, sl.bytes) != cudaSuccess || cudaMallocHost(&ctx->h_status, sl.bytes) != cudaSuccess) {
         cudaGetLastError();
         return set_err(ctx, NNLBM_ERR_OOM, "allocation of the %zu-byte status block failed", sl.bytes);
@@ -1225,17 +1210,10 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
     // one memset restarts every group's step cursors (and, for a reduction, every case's sums)
     const StatusLayout sl(ctx->cases.size());
     CK(cudaMemsetAsync(ctx->d_status, 0, (flags & NNLBM_STEP_REDUCE) ? sl.err : sl.red, ctx->stream));
-    // a readback is published by the step kernels themselves (their last block copies the
-    // status words into the slot) unless a group runs the staged form
-    bool publish = (flags & NNLBM_STEP_READBACK) != 0;
-    for (const Group& g : ctx->groups) publish = publish && !g.staged;
-    const int slot = (ctx->rb_head + ctx->rb_count) % NNLBM_READBACK_SLOTS;
-    ctx->publish_slot = publish ? slot : -1;
     for (Group& g : ctx->groups) {
         int rc = run_group_steps(ctx, g, n_steps, flags, true, false);
-        if (rc != NNLBM_OK) { ctx->publish_slot = -1; return rc; }
+        if (rc != NNLBM_OK) return rc;
     }
-    ctx->publish_slot = -1;
     for (Case& c : ctx->cases) {
         if (c.sched.empty()) continue;
         // consume the rows that were used; the last row stays in force
@@ -1244,8 +1222,12 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
         else c.sched.erase(c.sched.begin(), c.sched.end() - 3);
     }
     if (flags & NNLBM_STEP_READBACK) {
-        nnlbm_ctx::Readback& r = ctx->rb[slot];
-        if (!publish) CK(cudaMemcpyAsync(r.h, ctx->d_status, sl.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        nnlbm_ctx::Readback& r = ctx->rb[(ctx->rb_head + ctx->rb_count) % NNLBM_READBACK_SLOTS];
+        if (!r.h) {
+            CK(cudaMallocHost((void**)&r.h, sl.bytes));
+            CK(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+        }
+        CK(cudaMemcpyAsync(r.h, ctx->d_status, sl.bytes, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaEventRecord(r.done, ctx->stream));
         r.n = n_steps;
         r.parity = group_parities(ctx);

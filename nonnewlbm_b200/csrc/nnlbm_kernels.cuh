@@ -51,9 +51,7 @@ enum : int { L_FLUID = 0, L_WALL = 1, L_PERIODIC = 2, L_IN_L = 3, L_IN_R = 4, L_
 // of the node list
 enum : int { LF_SELF = 0x40, L_MASK = 0x0f };
 enum : int { CY_NONE = 0, CY_REF_FD = 1, CY_LOCAL_NEQ = 2 };
-// F_PUBLISH (the last step of a call with NNLBM_STEP_READBACK): the step kernel's last block
-// copies the group's status words into the host slot that StepCtl::pad names
-enum : int { F_STATS = 1, F_MACRO = 2, F_REDUCE = 4, F_PUBLISH = 16 };
+enum : int { F_STATS = 1, F_MACRO = 2, F_REDUCE = 4 };
 // macro field order of the context's macro array
 enum : int { M_RHO = 0, M_VX, M_VY, M_VZ, M_FX, M_FY, M_FZ, M_S11, M_S12, M_S13, M_S22, M_S32, M_S33, M_N };
 
@@ -193,10 +191,6 @@ struct GroupArgs {
     // test can make every wait run out with all copies complete
     long long stage_wait_ns;
     int stage_pad, pad3;
-    // F_PUBLISH: the context's status block on the device and the host slots (pinned, mapped
-    // into the device's address space) its copies go to, in the same layout
-    const char* status_base;
-    char* rb_slots[4];
 };
 
 // where a kernel finds the arguments of case ci: the device array, the parameters indexed
@@ -925,34 +919,6 @@ __device__ __noinline__ void node_batch(const int2* nodes, int n_nodes, const Ca
     }
 }
 
-// F_PUBLISH: the block that finishes last (a ticket in the group's spare cursor word, taken
-// after a fence that makes the block's sums and flags visible) copies the group's step
-// cursors and its cases' FP64 sums and watchdog words from the status block into the host
-// slot.  The host reads the slot once the step's event has completed, with no copy of its
-// own in the stream.
-template <class CT>
-__device__ __forceinline__ void publish_status(const GroupArgs<CT>& g, int slot)
-{
-    __shared__ int last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(g.cursor + 2, 1) == (int)gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    char* dst = g.rb_slots[slot & 3];
-    const int t = threadIdx.x;
-    if (t < 2) *(int*)(dst + ((const char*)(g.cursor + t) - g.status_base)) = __ldcg(g.cursor + t);
-    for (int j = 0; j < g.n_cases; ++j) {
-        const CaseArgs<CT>& a = g.cases[j];
-        double* red = (double*)(dst + ((const char*)a.red - g.status_base));
-        for (int i = t; i < 8 * kRedStripes; i += blockDim.x) red[i] = __ldcg(a.red + i);
-        if (t == 0) *(int*)(dst + ((const char*)a.err - g.status_base)) = __ldcg(a.err);
-    }
-}
-
 // the step kernel: one warp per chunk of the work list (per two chunks where the variant
 // pairs them), then one warp per 32 boundary nodes.  Both write only the slots their own
 // cells read, so they run side by side.
@@ -1003,7 +969,6 @@ __global__ void __launch_bounds__(256) __maxnreg__((StepRegs<DT, COL, PAIR>::val
             node_batch<DT, ODD>(g.nodes, g.n_nodes, g.cases, g.bc_prof, g.bc_buf, (w - g.n_chunks) * 32 + lane, step, flags);
         }
     }
-    if (flags & F_PUBLISH) publish_status(g, case_args<ARGS>(g, 0).ctl[step].pad);
 }
 
 // ---------------------------------------------------------------------------------------
