@@ -499,6 +499,9 @@ __host__ __device__ constexpr bool pairs_chunks(int dt, int col)
 #ifndef NNLBM_PAIR_REGS
 #define NNLBM_PAIR_REGS 128
 #endif
+#ifndef NNLBM_KBC_REGS
+#define NNLBM_KBC_REGS 128
+#endif
 #ifndef NNLBM_CHUNK_REGS
 #define NNLBM_CHUNK_REGS 64
 #endif
@@ -517,7 +520,7 @@ __host__ __device__ constexpr bool pairs_chunks(int dt, int col)
 template <int DT, int COL, bool PAIR>
 struct StepRegs {
     static constexpr int value = DT == 0                ? 255
-                                 : !pairs_chunks(DT, COL) ? 128
+                                 : !pairs_chunks(DT, COL) ? NNLBM_KBC_REGS
                                  : PAIR                   ? NNLBM_PAIR_REGS
                                  : DT == 1                ? NNLBM_CHUNK_REGS_F32
                                  : COL == COL_CUM         ? NNLBM_CHUNK_REGS_CUM16
