@@ -491,6 +491,40 @@ __device__ __forceinline__ void collide_bgk(CT* f, CT rho, CT ux, CT uy, CT uz, 
     }
 }
 
+// BGK of one cell in single precision with the populations of the planes x = -1 and x = 0
+// packed into f2 pairs (the same operations in the same order as collide_bgk; the x = +1
+// plane runs scalar)
+__device__ __forceinline__ void collide_bgk_packed(float* f, float rho, float ux, float uy, float uz, float fx, float fy,
+                                                   float fz, float nu)
+{
+    const float om = 1.f / (3.f * nu + 0.5f);
+    const float ir = 1.f / rho;
+    const float k = 1.f - 0.5f * om;
+    const FactEq<float> E(ux, uy, uz);
+    const f2 rX(-rho * E.X[0], -rho * E.X[1]);
+    const float rX2 = -rho * E.X[2];
+    const f2 A((-1.f - ux) * fx, (0.f - ux) * fx);
+    const float A2 = (1.f - ux) * fx;
+    const f2 om2(om), k2(k), three(3.0), ir2(ir);
+#pragma unroll
+    for (int iy = 0; iy < 3; ++iy)
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+            const int j = 3 * iy + iz;
+            const float Y = E.Y[iy], Z = E.Z[iz];
+            const float B = ((float)(iy - 1) - uy) * fy, C = ((float)(iz - 1) - uz) * fz;
+            const f2 feq = (rX * f2(Y, Y)) * f2(Z, Z);
+            const f2 src = (three * ((A + f2(B, B)) + f2(C, C))) * ir2;
+            const f2 fv(f[j], f[9 + j]);
+            const f2 nv = fv + mad(feq - fv, om2, (k2 * src) * feq);
+            f[j] = nv.v.x;
+            f[9 + j] = nv.v.y;
+            const float feq1 = (rX2 * Y) * Z;
+            const float src1 = (3.f * ((A2 + B) + C)) * ir;
+            f[18 + j] += (feq1 - f[18 + j]) * om + (k * src1) * feq1;
+        }
+}
+
 // MRT_LES, solver/lbm3d/lbm_col_mrt.h:12-78: second moments relaxed with a Smagorinsky rate,
 // everything rebuilt as w_q [rho (1 + 3 c.u) + 9/2 (c c - I/3) : (P - rho I/3)] form
 template <class CT>
@@ -681,6 +715,10 @@ __device__ __forceinline__ void step_cell(CT* f, CT fx, CT fy, CT fz, CT nu, con
 {
     if constexpr (COL == COL_CUM && PACK && NNLBM_CUM_PACKED && std::is_same<CT, float>::value) {
         step_cell_cum_packed(f, fx, fy, fz, nu, cy, S, rho, ux, uy, uz);
+    } else if constexpr (COL == COL_BGK && PACK && std::is_same<CT, float>::value) {
+        density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
+        if (cy) nu = local_nu<CT, PT>(f, rho, ux, uy, uz, *cy, S);
+        collide_bgk_packed(f, rho, ux, uy, uz, fx, fy, fz, nu);
     } else if constexpr (COL == COL_CUM) {
         cum_columns<CT>(f);
         cum_density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
