@@ -584,7 +584,7 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         // a runtime branch inside it)
         CT Sl[6];
         const CYParams<CT> cy = {a.nu, a.nu0, a.lam, a.a, a.n};
-        step_cell<CT, COL, CT, NNLBM_PACK_DT(DT)>(f, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl, rho, ux, uy, uz);
+        step_cell<CT, COL, CT, NNLBM_PACK_DT(DT) ? DT : 0>(f, fx, fy, fz, a.nu, a.cy_mode == CY_LOCAL_NEQ ? &cy : nullptr, Sl, rho, ux, uy, uz);
         // the gather of this step reads the slots written below
         pdl_wait();
         T* ps = (T*)a.df + c;

@@ -527,10 +527,12 @@ __device__ __forceinline__ void collide_bgk_packed(float* f, float rho, float ux
 
 // MRT_LES, solver/lbm3d/lbm_col_mrt.h:12-78: second moments relaxed with a Smagorinsky rate,
 // everything rebuilt as w_q [rho (1 + 3 c.u) + 9/2 (c c - I/3) : (P - rho I/3)] form
+// the relaxed second moments of MRT_LES (P, and tr = trace P) from the populations
 template <class CT>
-__device__ __forceinline__ void collide_mrt(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu)
+__device__ __forceinline__ void mrt_moments(const CT* f, CT rho, CT ux, CT uy, CT uz, CT nu, CT& Pxx, CT& Pyy, CT& Pzz, CT& Pxy,
+                                            CT& Pxz, CT& Pyz, CT& tr)
 {
-    CT Pxx = CT(0), Pyy = CT(0), Pzz = CT(0), Pxy = CT(0), Pxz = CT(0), Pyz = CT(0);
+    Pxx = CT(0); Pyy = CT(0); Pzz = CT(0); Pxy = CT(0); Pxz = CT(0); Pyz = CT(0);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const int cx = cxq(q), cy = cyq(q), cz = czq(q);
@@ -552,7 +554,14 @@ __device__ __forceinline__ void collide_mrt(CT* f, CT rho, CT ux, CT uy, CT uz, 
     const CT om = CT(2) / (dsqrt<CT>(tau * tau + CT(2) * CT(0.0342) * CT(9) * dsqrt<CT>(Qs) / rho) + tau);
     Pxx -= om * Pnxx; Pyy -= om * Pnyy; Pzz -= om * Pnzz;
     Pxy -= om * Pnxy; Pxz -= om * Pnxz; Pyz -= om * Pnyz;
-    const CT tr = Pxx + Pyy + Pzz;
+    tr = Pxx + Pyy + Pzz;
+}
+
+template <class CT>
+__device__ __forceinline__ void collide_mrt(CT* f, CT rho, CT ux, CT uy, CT uz, CT nu)
+{
+    CT Pxx, Pyy, Pzz, Pxy, Pxz, Pyz, tr;
+    mrt_moments<CT>(f, rho, ux, uy, uz, nu, Pxx, Pyy, Pzz, Pxy, Pxz, Pyz, tr);
 #pragma unroll
     for (int q = 0; q < 27; ++q) {
         const int cx = cxq(q), cy = cyq(q), cz = czq(q);
@@ -562,6 +571,37 @@ __device__ __forceinline__ void collide_mrt(CT* f, CT rho, CT ux, CT uy, CT uz, 
                       + CT(2) * (CT(cx * cy) * Pxy + CT(cx * cz) * Pxz + CT(cy * cz) * Pyz);
         f[q] = weight<CT>(q) * (rho * (CT(2.5) - CT(1.5) * CT(c2) + CT(3) * cu) + CT(4.5) * pp - CT(1.5) * tr);
     }
+}
+
+// MRT_LES of one cell in single precision, its rebuild with the planes x = -1 and x = 0 as
+// packed f2 pairs (the terms without c_x are shared by the pair; the x = +1 plane runs
+// scalar)
+__device__ __forceinline__ void collide_mrt_packed(float* f, float rho, float ux, float uy, float uz, float nu)
+{
+    float Pxx, Pyy, Pzz, Pxy, Pxz, Pyz, tr;
+    mrt_moments<float>(f, rho, ux, uy, uz, nu, Pxx, Pyy, Pzz, Pxy, Pxz, Pyz, tr);
+    const f2 rho2(rho, rho), ux0(-ux, 0.f), three(3.0), p45(4.5), tr15(1.5f * tr, 1.5f * tr);
+#pragma unroll
+    for (int iy = 0; iy < 3; ++iy)
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+            const int cy = iy - 1, cz = iz - 1, j = 3 * iy + iz;
+            const float s_cu = (float)cy * uy + (float)cz * uz;
+            const float s_pp = (float)(cy * cy) * Pyy + (float)(cz * cz) * Pzz + 2.f * (float)(cy * cz) * Pyz;
+            const float x_pp = 2.f * ((float)cy * Pxy + (float)cz * Pxz);
+            const int s_c2 = cy * cy + cz * cz;
+            // x = -1 (c_x^2 = 1) and x = 0
+            const f2 cu = ux0 + f2(s_cu, s_cu);
+            const f2 pp = f2(Pxx - x_pp, 0.f) + f2(s_pp, s_pp);
+            const f2 k(2.5f - 1.5f * (float)(1 + s_c2), 2.5f - 1.5f * (float)s_c2);
+            const f2 w(weight<float>(j), weight<float>(9 + j));
+            const f2 v = w * (mad(rho2, mad(three, cu, k), p45 * pp) - tr15);
+            f[j] = v.v.x;
+            f[9 + j] = v.v.y;
+            // x = +1
+            const float cu1 = ux + s_cu, pp1 = Pxx + x_pp + s_pp;
+            f[18 + j] = weight<float>(18 + j) * (rho * (2.5f - 1.5f * (float)(1 + s_c2) + 3.f * cu1) + 4.5f * pp1 - 1.5f * tr);
+        }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -708,14 +748,22 @@ __device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT f
 // the cumulant the first half of the forward transform's z pass sums the populations by
 // column, and the density and momentum come from those sums instead of separate sums over
 // all 27
-// PACK: the one-cell cumulant in single precision uses step_cell_cum_packed
-template <class CT, int COL, class PT = CT, bool PACK = false>
+// PACK_DT: the storage type of a one-cell step in single precision (0: none), which picks the
+// forms with the planes x = -1, 0 as packed pairs: the cumulant and BGK with every
+// single-precision storage, MRT_LES with 16-bit storage (with FP32 storage, bound by HBM,
+// the packed rebuild measured 1 % slower)
+template <class CT, int COL, class PT = CT, int PACK_DT = 0>
 __device__ __forceinline__ void step_cell(CT* f, CT fx, CT fy, CT fz, CT nu, const CYParams<PT>* cy, CT* S, CT& rho, CT& ux,
                                           CT& uy, CT& uz)
 {
-    if constexpr (COL == COL_CUM && PACK && NNLBM_CUM_PACKED && std::is_same<CT, float>::value) {
+    constexpr bool PACK = PACK_DT != 0 && std::is_same<CT, float>::value;
+    if constexpr (COL == COL_CUM && PACK && NNLBM_CUM_PACKED) {
         step_cell_cum_packed(f, fx, fy, fz, nu, cy, S, rho, ux, uy, uz);
-    } else if constexpr (COL == COL_BGK && PACK && std::is_same<CT, float>::value) {
+    } else if constexpr (COL == COL_MRT && PACK && PACK_DT >= 2) {
+        density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
+        if (cy) nu = local_nu<CT, PT>(f, rho, ux, uy, uz, *cy, S);
+        collide_mrt_packed(f, rho, ux, uy, uz, nu);
+    } else if constexpr (COL == COL_BGK && PACK) {
         density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
         if (cy) nu = local_nu<CT, PT>(f, rho, ux, uy, uz, *cy, S);
         collide_bgk_packed(f, rho, ux, uy, uz, fx, fy, fz, nu);
