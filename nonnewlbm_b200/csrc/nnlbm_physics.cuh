@@ -491,6 +491,24 @@ __device__ __forceinline__ void collide_bgk(CT* f, CT rho, CT ux, CT uy, CT uz, 
     }
 }
 
+// density and velocity of one cell in single precision from its column sums (the z pass's
+// first half, cum_columns, with the columns of the planes x = -1, 0 as packed pairs), f
+// unchanged
+__device__ __forceinline__ void packed_density_velocity(const float* f, float fx, float fy, float fz, float& rho, float& ux,
+                                                        float& uy, float& uz)
+{
+    float k[27];
+#pragma unroll
+    for (int iy = 0; iy < 3; ++iy) {
+        const f2 m(f[3 * iy], f[9 + 3 * iy]), z(f[3 * iy + 1], f[9 + 3 * iy + 1]), p(f[3 * iy + 2], f[9 + 3 * iy + 2]);
+        const f2 d = p - m, c0 = (p + m) + z;
+        const float mq = f[18 + 3 * iy], zq = f[18 + 3 * iy + 1], pq = f[18 + 3 * iy + 2];
+        k[3 * iy] = c0.v.x; k[9 + 3 * iy] = c0.v.y; k[18 + 3 * iy] = (pq + mq) + zq;
+        k[3 * iy + 1] = d.v.x; k[9 + 3 * iy + 1] = d.v.y; k[18 + 3 * iy + 1] = pq - mq;
+    }
+    cum_density_velocity<float>(k, fx, fy, fz, rho, ux, uy, uz);
+}
+
 // BGK of one cell in single precision with the populations of the planes x = -1 and x = 0
 // packed into f2 pairs (the same operations in the same order as collide_bgk; the x = +1
 // plane runs scalar)
@@ -751,7 +769,8 @@ __device__ __forceinline__ void collide(CT* f, CT rho, CT ux, CT uy, CT uz, CT f
 // PACK_DT: the storage type of a one-cell step in single precision (0: none), which picks the
 // forms with the planes x = -1, 0 as packed pairs: the cumulant and BGK with every
 // single-precision storage, MRT_LES with 16-bit storage (with FP32 storage, bound by HBM,
-// the packed rebuild measured 1 % slower)
+// the packed rebuild measured 1 % slower).  KBC keeps the scalar sums: at its 128 registers
+// the packed ones spill and measured 5 % slower
 template <class CT, int COL, class PT = CT, int PACK_DT = 0>
 __device__ __forceinline__ void step_cell(CT* f, CT fx, CT fy, CT fz, CT nu, const CYParams<PT>* cy, CT* S, CT& rho, CT& ux,
                                           CT& uy, CT& uz)
@@ -760,11 +779,11 @@ __device__ __forceinline__ void step_cell(CT* f, CT fx, CT fy, CT fz, CT nu, con
     if constexpr (COL == COL_CUM && PACK && NNLBM_CUM_PACKED) {
         step_cell_cum_packed(f, fx, fy, fz, nu, cy, S, rho, ux, uy, uz);
     } else if constexpr (COL == COL_MRT && PACK && PACK_DT >= 2) {
-        density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
+        packed_density_velocity(f, fx, fy, fz, rho, ux, uy, uz);
         if (cy) nu = local_nu<CT, PT>(f, rho, ux, uy, uz, *cy, S);
         collide_mrt_packed(f, rho, ux, uy, uz, nu);
     } else if constexpr (COL == COL_BGK && PACK) {
-        density_velocity<CT>(f, fx, fy, fz, rho, ux, uy, uz);
+        packed_density_velocity(f, fx, fy, fz, rho, ux, uy, uz);
         if (cy) nu = local_nu<CT, PT>(f, rho, ux, uy, uz, *cy, S);
         collide_bgk_packed(f, rho, ux, uy, uz, fx, fy, fz, nu);
     } else if constexpr (COL == COL_CUM) {
