@@ -59,6 +59,36 @@ def test_pipelined_readback_matches_synchronous_steps(n_cases):
         assert np.array_equal(sync.stats(k)[0], pipe.stats(k)[0])
 
 
+def test_pipelined_readback_two_launch_groups():
+    """A context of two launch groups (cumulant and BGK): each group's cursors are checked at
+    its own parity, and the sums match synchronous steps."""
+    wall = small_junction()
+    nz, ny, nx = wall.shape
+    def make():
+        lat = Lattice([CaseSpec((nx, ny, nz), dtype="f32", collision=col, nu=0.02) for col in ("CUM", "BGK")])
+        areas = []
+        for k in range(2):
+            c = lat.setup_tcpc(wall, ic=k)
+            areas.append((c["left_area"], c["right_area"]))
+        lat.init_equilibrium()
+        return lat, areas
+    sync, areas = make()
+    pipe, _ = make()
+    expect, got = [], []
+    for step in range(7):
+        for k in range(2):
+            sync.set_schedule(_row(areas, k, step), ic=k)
+            pipe.set_schedule(_row(areas, k, step), ic=k)
+        sync.step(1, reduce=True)
+        expect.append(np.array([sync.reduce(k) for k in range(2)]))
+        pipe.step(1, reduce=True, wait=False, readback=True)
+        if step > 0:
+            got.append(pipe.readback())
+    got.append(pipe.readback())
+    for e, g in zip(expect, got):
+        assert np.array_equal(e, g)
+
+
 def test_readback_refusals():
     lat, _ = _lattice()
     with pytest.raises(capi.NnlbmError):
