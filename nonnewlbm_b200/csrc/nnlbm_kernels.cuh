@@ -527,6 +527,20 @@ struct StepRegs {
                                                           : NNLBM_CHUNK_REGS;
 };
 
+// a 16-bit stored value as float, and a float rounded to the 16-bit storage type
+template <int DT>
+__device__ __forceinline__ float widen16(typename Storage<DT>::T v)
+{
+    if constexpr (DT == 2) return __half2float(v);
+    else return __bfloat162float(v);
+}
+template <int DT>
+__device__ __forceinline__ typename Storage<DT>::T narrow16(float v)
+{
+    if constexpr (DT == 2) return __float2half_rn(v);
+    else return __float2bfloat16_rn(v);
+}
+
 // ---------------------------------------------------------------------------------------
 // one 32-cell chunk of the fused step (solver/lbm3d/core.h:578-800), one warp, one cell per
 // lane.  The populations go straight from HBM to registers, 27 coalesced row loads per
@@ -561,7 +575,32 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         // halfway bounce-back: which neighbours are walls (CH_HW chunks, odd step only)
         const uint32_t hwm = (ODD && (ch.cflags & CH_HW)) ? a.hw[c] : 0u;
         CT f[27];
-        if (!ODD) {
+        // PAIR16: 16-bit storage with BGK (measured +2 %; the cumulant measured 3 % slower): the
+        // planes x = -1 and x = 0 scale and shift as packed pairs on the way in and out
+        constexpr bool PAIR16 = DT >= 2 && COL == COL_BGK;
+        if constexpr (PAIR16) {
+            if (!ODD || plain) {
+                // slot q at c, or slot opp(q) at c - c_q
+                auto src = [&](int q) { return (const T*)(ODD ? odd_ld(a, q) : a.slot_even[q]) + c; };
+                const f2 isc2(a.inv_scale, a.inv_scale);
+#pragma unroll
+                for (int j = 0; j < 9; ++j) {
+                    const f2 v = mad(f2(widen16<DT>(*src(j)), widen16<DT>(*src(9 + j))), isc2,
+                                     f2(weight<float>(j), weight<float>(9 + j)));
+                    f[j] = v.v.x;
+                    f[9 + j] = v.v.y;
+                }
+#pragma unroll
+                for (int q = 18; q < 27; ++q) f[q] = S::from(*src(q), q, a.inv_scale);
+            }
+        }
+        if constexpr (PAIR16) {
+            if (ODD && !plain) {
+#pragma unroll
+                for (int q = 0; q < 27; ++q)
+                    f[q] = S::from(((hwm >> oppq(q)) & 1u) ? pc[q * qs] : pc[oppq(q) * qs + nbr(q, -1)], q, a.inv_scale);
+            }
+        } else if (!ODD) {
             // slot q at c
 #pragma unroll
             for (int q = 0; q < 27; ++q) f[q] = S::from(((const T*)a.slot_even[q])[c], q, a.inv_scale);
@@ -588,7 +627,25 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         // the gather of this step reads the slots written below
         pdl_wait();
         T* ps = (T*)a.df + c;
-        if (!ODD) {
+        if constexpr (PAIR16) {
+            if (!ODD || plain) {
+                // slot opp(q) at c, or slot q at c + c_q
+                auto dst = [&](int q) { return (T*)(ODD ? a.slot_odd_st[q] : a.slot_even[oppq(q)]) + c; };
+                const f2 sc2(a.scale, a.scale);
+#pragma unroll
+                for (int j = 0; j < 9; ++j) {
+                    const f2 v = mad(f2(f[j], f[9 + j]), sc2, f2(-(weight<float>(j) * a.scale), -(weight<float>(9 + j) * a.scale)));
+                    *dst(j) = narrow16<DT>(v.v.x);
+                    *dst(9 + j) = narrow16<DT>(v.v.y);
+                }
+#pragma unroll
+                for (int q = 18; q < 27; ++q) S::store(dst(q), 0, q, f[q], a.scale);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 27; ++q)
+                    S::store(ps, ((hwm >> q) & 1u) ? oppq(q) * qs : q * qs + nbr(q, 1), q, f[q], a.scale);
+            }
+        } else if (!ODD) {
             // slot opp(q) at c
 #pragma unroll
             for (int q = 0; q < 27; ++q) S::store((T*)a.slot_even[oppq(q)], c, q, f[q], a.scale);
