@@ -575,9 +575,10 @@ __device__ __forceinline__ void fluid_chunk(const CaseArgs<typename Storage<DT>:
         // halfway bounce-back: which neighbours are walls (CH_HW chunks, odd step only)
         const uint32_t hwm = (ODD && (ch.cflags & CH_HW)) ? a.hw[c] : 0u;
         CT f[27];
-        // PAIR16: 16-bit storage with BGK (measured +2 %; the cumulant measured 3 % slower): the
+        // PAIR16: 16-bit storage with BGK or MRT (measured +2 % each; the cumulant measured 3 %
+        // slower): the
         // planes x = -1 and x = 0 scale and shift as packed pairs on the way in and out
-        constexpr bool PAIR16 = DT >= 2 && COL == COL_BGK;
+        constexpr bool PAIR16 = DT >= 2 && (COL == COL_BGK || COL == COL_MRT);
         if constexpr (PAIR16) {
             if (!ODD || plain) {
                 // slot q at c, or slot opp(q) at c - c_q
