@@ -96,7 +96,9 @@ enum {
     NNLBM_STEP_READBACK = 16 /* with NNLBM_STEP_ASYNC only: after the steps, also enqueue a copy of
                               the context's status block (step cursors, watchdog flags, the FP64
                               sums of NNLBM_STEP_REDUCE) into the next of NNLBM_READBACK_SLOTS
-                              pinned host slots, for nnlbm_readback */
+                              mapped pinned host slots, for nnlbm_readback.  A one-block kernel
+                              in the context's stream writes the slot (NNLBM_READBACK_COPY=1 in
+                              the environment at nnlbm_create: a device-to-host copy instead) */
 };
 #define NNLBM_READBACK_SLOTS 4
 
