@@ -222,6 +222,7 @@ struct nnlbm_ctx {
     Readback rb[NNLBM_READBACK_SLOTS];
     int rb_head = 0, rb_count = 0;
     bool rb_copy = false;  // NNLBM_READBACK_COPY=1: a device-to-host copy instead of k_publish_status
+    bool prologue_copy = false;  // NNLBM_PROLOGUE_COPY=1: copy and memsets instead of k_step_prologue
     // the staged step's bounded waits (GroupArgs::stage_wait_ns, stage_pad)
     long long stage_wait_ns = 2000000000LL;
     int stage_pad = 0;
@@ -576,6 +577,25 @@ int ensure_graphs(nnlbm_ctx* ctx, Group& g)
     return NNLBM_OK;
 }
 
+// a call's new control rows, carried in the launch's parameters, plus the zeroing of the case's
+// FP64 sums and the group's step cursors: one kernel before the step, where a host-to-device copy
+// and two memsets were three operations
+constexpr int kPutRowWords = 64;  // 512 B of control rows: 16 FP32 steps or 9 FP64 steps
+struct CtlRows {
+    unsigned long long w[kPutRowWords];
+};
+__global__ void __launch_bounds__(256) k_step_prologue(const __grid_constant__ CtlRows rows, int words,
+                                                       unsigned long long* __restrict__ ctl,
+                                                       unsigned long long* __restrict__ red, int red_words,
+                                                       int* __restrict__ cursors)
+{
+    const int t = threadIdx.x;
+    if (t < words) ctl[t] = rows.w[t];
+    if (red)
+        for (int i = t; i < red_words; i += blockDim.x) red[i] = 0ull;
+    if (cursors && t < 2) cursors[t] = 0;
+}
+
 // host side of one nnlbm_step call for every case of a group, up to the launches
 // `reset`: clear the group's step cursors (and its cases' sums for NNLBM_STEP_REDUCE); a
 // caller that cleared the whole status block already passes false
@@ -584,6 +604,7 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = t
     int rc;
     int64_t parity = -1;
     ctx->status_fresh = false;
+    bool ints_zeroed = false;
     for (int ic : g.cases) {
         Case& c = ctx->cases[ic];
         if (!c.has_map || !c.has_state) return set_err(ctx, NNLBM_ERR_ARG, "case %d has no map or initial state", ic);
@@ -600,8 +621,26 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = t
         if (c.ct_bytes == 8) fill_ctl<double>(c, buf, n, flags);
         else fill_ctl<float>(c, buf, n, flags);
         // rows already on the device (a constant inflow stepped call after call) are not sent again;
-        // new ones go through a pinned staging buffer, reused once its last copy has completed
-        if (buf.size() > c.ctl_dev.size() || memcmp(buf.data(), c.ctl_dev.data(), buf.size()) != 0) {
+        // a few new ones travel in the parameters of k_step_prologue, more go through a pinned
+        // staging buffer, reused once its last copy has completed
+        const bool send = buf.size() > c.ctl_dev.size() || memcmp(buf.data(), c.ctl_dev.data(), buf.size()) != 0;
+        const bool zero_red = reset && (flags & NNLBM_STEP_REDUCE);
+        const bool small = buf.size() % 8 == 0 && buf.size() <= sizeof(CtlRows);
+        if (!ctx->prologue_copy && (zero_red || (reset && !ints_zeroed) || (send && small))) {
+            CtlRows rows;
+            const int words = (send && small) ? (int)(buf.size() / 8) : 0;
+            if (words) memcpy(rows.w, buf.data(), buf.size());
+            int* cursors = (reset && !ints_zeroed) ? g.d_ints : nullptr;
+            k_step_prologue<<<1, 256, 0, ctx->stream>>>(rows, words, (unsigned long long*)c.d_ctl,
+                                                         zero_red ? (unsigned long long*)c.d_red : nullptr,
+                                                         (int)(kRedBytes / 8), cursors);
+            CK(cudaGetLastError());
+            ints_zeroed = ints_zeroed || cursors;
+            if (words) c.ctl_dev = buf;
+        } else if (zero_red) {
+            CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
+        }
+        if (send && (ctx->prologue_copy || !small)) {
             const int k = c.ctl_slot;
             c.ctl_slot = (k + 1) % Case::kCtlSlots;
             if (!c.ctl_done[k]) CK(cudaEventCreateWithFlags(&c.ctl_done[k], cudaEventDisableTiming));
@@ -618,10 +657,9 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = t
             CK(cudaEventRecord(c.ctl_done[k], ctx->stream));
             c.ctl_dev = buf;
         }
-        if (reset && (flags & NNLBM_STEP_REDUCE)) CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
     }
     if ((rc = prepare_group(ctx, g)) != NNLBM_OK) return rc;
-    if (reset) CK(cudaMemsetAsync(g.d_ints, 0, 2 * sizeof(int), ctx->stream));
+    if (reset && !ints_zeroed) CK(cudaMemsetAsync(g.d_ints, 0, 2 * sizeof(int), ctx->stream));
     return NNLBM_OK;
 }
 
@@ -922,6 +960,7 @@ int nnlbm_create(const nnlbm_case_desc* desc, int n_cases, int device, nnlbm_ctx
     // a test's stall of the staged step: every wait expects 16 bytes that never arrive and
     // gives up after a millisecond (NNLBM_ERR_TIMEOUT); all its copies still complete
     if (const char* t = getenv("NNLBM_READBACK_COPY"); t && atoi(t) == 1) ctx->rb_copy = true;
+    if (const char* t = getenv("NNLBM_PROLOGUE_COPY"); t && atoi(t) == 1) ctx->prologue_copy = true;
     if (const char* t = getenv("NNLBM_TEST_STAGE_STALL"); t && atoi(t) == 1) {
         ctx->stage_wait_ns = 1000000LL;
         ctx->stage_pad = 16;
