@@ -223,6 +223,9 @@ struct nnlbm_ctx {
     int rb_head = 0, rb_count = 0;
     bool rb_copy = false;  // NNLBM_READBACK_COPY=1: a device-to-host copy instead of k_publish_status
     bool prologue_copy = false;  // NNLBM_PROLOGUE_COPY=1: copy and memsets instead of k_step_prologue
+    // a status range that the next k_step_prologue clears (left by nnlbm_step for its first launch)
+    unsigned long long* zero_next = nullptr;
+    int zero_next_words = 0;
     // the staged step's bounded waits (GroupArgs::stage_wait_ns, stage_pad)
     long long stage_wait_ns = 2000000000LL;
     int stage_pad = 0;
@@ -577,22 +580,22 @@ int ensure_graphs(nnlbm_ctx* ctx, Group& g)
     return NNLBM_OK;
 }
 
-// a call's new control rows, carried in the launch's parameters, plus the zeroing of the case's
-// FP64 sums and the group's step cursors: one kernel before the step, where a host-to-device copy
-// and two memsets were three operations
+// a call's new control rows, carried in the launch's parameters, plus the zeroing of a status
+// range (the call's step cursors and sums, or one case's sums) and of the group's step cursors:
+// one kernel before the step, where a host-to-device copy and memsets were separate operations
 constexpr int kPutRowWords = 64;  // 512 B of control rows: 16 FP32 steps or 9 FP64 steps
 struct CtlRows {
     unsigned long long w[kPutRowWords];
 };
 __global__ void __launch_bounds__(256) k_step_prologue(const __grid_constant__ CtlRows rows, int words,
                                                        unsigned long long* __restrict__ ctl,
-                                                       unsigned long long* __restrict__ red, int red_words,
+                                                       unsigned long long* __restrict__ zero, int zero_words,
                                                        int* __restrict__ cursors)
 {
     const int t = threadIdx.x;
     if (t < words) ctl[t] = rows.w[t];
-    if (red)
-        for (int i = t; i < red_words; i += blockDim.x) red[i] = 0ull;
+    if (zero)
+        for (int i = t; i < zero_words; i += blockDim.x) zero[i] = 0ull;
     if (cursors && t < 2) cursors[t] = 0;
 }
 
@@ -626,21 +629,33 @@ int prepare_steps(nnlbm_ctx* ctx, Group& g, int64_t n, int flags, bool reset = t
         const bool send = buf.size() > c.ctl_dev.size() || memcmp(buf.data(), c.ctl_dev.data(), buf.size()) != 0;
         const bool zero_red = reset && (flags & NNLBM_STEP_REDUCE);
         const bool small = buf.size() % 8 == 0 && buf.size() <= sizeof(CtlRows);
-        if (!ctx->prologue_copy && (zero_red || (reset && !ints_zeroed) || (send && small))) {
+        // new rows that fit go in the parameters of k_step_prologue, which also clears the status
+        // range nnlbm_step left for the first launch (else this case's sums) and the group's
+        // cursors; without new rows the clearing stays with memsets (cheaper than a launch)
+        const bool put = !ctx->prologue_copy && send && small;
+        if (put) {
+            unsigned long long* zero = ctx->zero_next ? ctx->zero_next : zero_red ? (unsigned long long*)c.d_red : nullptr;
+            const int zero_words = ctx->zero_next ? ctx->zero_next_words : (int)(kRedBytes / 8);
+            if (ctx->zero_next && zero_red) CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
             CtlRows rows;
-            const int words = (send && small) ? (int)(buf.size() / 8) : 0;
-            if (words) memcpy(rows.w, buf.data(), buf.size());
+            memcpy(rows.w, buf.data(), buf.size());
             int* cursors = (reset && !ints_zeroed) ? g.d_ints : nullptr;
-            k_step_prologue<<<1, 256, 0, ctx->stream>>>(rows, words, (unsigned long long*)c.d_ctl,
-                                                         zero_red ? (unsigned long long*)c.d_red : nullptr,
-                                                         (int)(kRedBytes / 8), cursors);
+            k_step_prologue<<<1, 256, 0, ctx->stream>>>(rows, (int)(buf.size() / 8), (unsigned long long*)c.d_ctl, zero,
+                                                         zero_words, cursors);
             CK(cudaGetLastError());
+            ctx->zero_next = nullptr;
+            ctx->zero_next_words = 0;
             ints_zeroed = ints_zeroed || cursors;
-            if (words) c.ctl_dev = buf;
-        } else if (zero_red) {
-            CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
+            c.ctl_dev = buf;
+        } else {
+            if (ctx->zero_next) {
+                CK(cudaMemsetAsync(ctx->zero_next, 0, (size_t)ctx->zero_next_words * 8, ctx->stream));
+                ctx->zero_next = nullptr;
+                ctx->zero_next_words = 0;
+            }
+            if (zero_red) CK(cudaMemsetAsync(c.d_red, 0, kRedBytes, ctx->stream));
         }
-        if (send && (ctx->prologue_copy || !small)) {
+        if (send && !put) {
             const int k = c.ctl_slot;
             c.ctl_slot = (k + 1) % Case::kCtlSlots;
             if (!c.ctl_done[k]) CK(cudaEventCreateWithFlags(&c.ctl_done[k], cudaEventDisableTiming));
@@ -1258,12 +1273,22 @@ int nnlbm_step(nnlbm_ctx* ctx, int64_t n_steps, int flags)
     if ((flags & NNLBM_STEP_READBACK) && ctx->rb_count == NNLBM_READBACK_SLOTS)
         return set_err(ctx, NNLBM_ERR_ARG, "%d status copies pending: call nnlbm_readback first", NNLBM_READBACK_SLOTS);
     CK(cudaSetDevice(ctx->device));
-    // one memset restarts every group's step cursors (and, for a reduction, every case's sums)
+    // every group's step cursors (and, for a reduction, every case's sums) restart from zero: the
+    // first group's first k_step_prologue clears them, or one memset
     const StatusLayout sl(ctx->cases.size());
-    CK(cudaMemsetAsync(ctx->d_status, 0, (flags & NNLBM_STEP_REDUCE) ? sl.err : sl.red, ctx->stream));
+    const size_t zero_bytes = (flags & NNLBM_STEP_REDUCE) ? sl.err : sl.red;
+    if (ctx->prologue_copy) {
+        CK(cudaMemsetAsync(ctx->d_status, 0, zero_bytes, ctx->stream));
+    } else {
+        ctx->zero_next = (unsigned long long*)ctx->d_status;
+        ctx->zero_next_words = (int)(zero_bytes / 8);
+    }
     for (Group& g : ctx->groups) {
         int rc = run_group_steps(ctx, g, n_steps, flags, true, false);
-        if (rc != NNLBM_OK) return rc;
+        if (rc != NNLBM_OK) {
+            ctx->zero_next = nullptr;
+            return rc;
+        }
     }
     for (Case& c : ctx->cases) {
         if (c.sched.empty()) continue;
