@@ -105,3 +105,27 @@ def test_readback_refusals():
         lat.readback()
     lat.step(2, reduce=True)  # synchronous steps go on as before
     assert np.isfinite(lat.reduce()).all()
+
+
+def test_copy_paths_match_kernel_paths(monkeypatch):
+    """NNLBM_PROLOGUE_COPY=1 and NNLBM_READBACK_COPY=1 (read at context creation) move the control
+    rows and the status block with copies instead of the prologue and publish kernels: the sums
+    and the populations are bitwise the same."""
+    n = 9
+    fast, areas = _lattice(2)
+    monkeypatch.setenv("NNLBM_PROLOGUE_COPY", "1")
+    monkeypatch.setenv("NNLBM_READBACK_COPY", "1")
+    copy, _ = _lattice(2)
+    got = {id(fast): [], id(copy): []}
+    for lat in (fast, copy):
+        for step in range(n):
+            for k in range(2):
+                lat.set_schedule(_row(areas, k, step), ic=k)
+            lat.step(1, stats=True, reduce=True, wait=False, readback=True)
+            if step > 0:
+                got[id(lat)].append(lat.readback())
+        got[id(lat)].append(lat.readback())
+    for a, b in zip(got[id(fast)], got[id(copy)]):
+        assert np.array_equal(a, b)
+    for k in range(2):
+        assert np.array_equal(fast.export_df(k), copy.export_df(k))
